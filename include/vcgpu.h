@@ -1,0 +1,144 @@
+/*
+ * vcgpu.h -- C ABI of the B200 exact vertex-cover solver (libvcgpu.so).
+ *
+ * The reference (GregorySchwing/Parallel-Vertex-Cover-Algorithms-on-GPUs) has no
+ * library API: its boundary is the `./output` command line plus one kernel
+ * launch per solve.  Each entry point below names the reference interface it
+ * replaces.  Plain pointers and sizes only; no CUDA or torch types appear in
+ * the signatures (a stream is passed as `void*`, a cudaStream_t).
+ *
+ * Ownership: every input is borrowed and never freed; outputs are caller-owned.
+ * Errors are returned as vc_status codes -- nothing here calls exit().
+ * Threading: calls are serialised per device inside the library; a server
+ * handle (vc_server_*) is used by one host thread at a time.
+ */
+#ifndef VCGPU_H
+#define VCGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vc_status {
+    VC_OK = 0,
+    VC_ERR_INVALID = 1,   /* bad argument or malformed graph */
+    VC_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    VC_ERR_NOMEM = 3,     /* device memory or the admission budget is exhausted */
+    VC_ERR_TOO_LARGE = 4, /* the graph exceeds what the kernels support */
+    VC_TIMEOUT = 5,       /* stopped at the time limit: size is an upper bound */
+    VC_BUDGET = 6,        /* stopped at the node limit: size is an upper bound */
+    VC_ERR_INTERNAL = 7,  /* a device-side consistency check failed */
+    VC_ERR_NO_DEVICE = 8, /* no usable CUDA device */
+    VC_PENDING = 9        /* server: the request is still running */
+} vc_status;
+
+typedef enum vc_instance {
+    VC_MVC = 0, /* minimum vertex cover (reference `-i mvc`, config.h:125-129) */
+    VC_PVC = 1  /* parameterized vertex cover, decision size <= k (`-i pvc -k K`) */
+} vc_instance;
+
+/* vc_request.flags */
+#define VC_FLAG_DEVICE_INPUT 0x1u /* vc_csr / arena pointers are device pointers */
+#define VC_FLAG_NO_VALIDATE 0x2u  /* skip the host-side CSR checks */
+
+/* One undirected simple graph in the reference's CSRGraph layout
+ * (src/CSRGraphRep.h:4-18): row_ptr = srcPtr[n+1], col = dst[2m] with every
+ * edge stored in both directions and each row sorted ascending
+ * (src/auxFunctions.cpp:203-206); degree (optional, may be NULL) must equal
+ * row_ptr[v+1]-row_ptr[v].  Ids are 0-based. */
+typedef struct vc_csr {
+    uint32_t n;
+    uint32_t m;
+    const uint32_t *row_ptr;
+    const uint32_t *col;
+    const int32_t *degree;
+} vc_csr;
+
+/* Many graphs packed into one arena: graph i has n[i] vertices, its n[i]+1
+ * local row offsets start at row_ptr[row_off[i]] and its neighbour ids at
+ * col[col_off[i]]. */
+typedef struct vc_csr_arena {
+    uint32_t count;
+    const uint32_t *n;
+    const uint64_t *row_off;
+    const uint64_t *col_off;
+    const uint32_t *row_ptr;
+    const uint32_t *col;
+} vc_csr_arena;
+
+/* What to solve.  `ub` plays the role of the reference's `minimum` argument
+ * (main.cu:73 / Sequential(graph, minimum)): when nonzero the search only looks
+ * for covers of size <= ub, and size = min(ub, OPT) like the reference returns;
+ * 0 means no bound.  node_limit / time_limit_s stop a search early (status
+ * VC_BUDGET / VC_TIMEOUT); 0 means unlimited / the library default (300 s). */
+typedef struct vc_request {
+    uint32_t instance;   /* vc_instance */
+    uint32_t k;          /* PVC parameter (reference -k) */
+    uint32_t ub;
+    uint32_t flags;      /* VC_FLAG_* */
+    uint64_t node_limit;
+    double time_limit_s;
+    int32_t device;      /* CUDA ordinal, -1 = current device */
+    uint32_t reserved;
+    void *stream;        /* cudaStream_t to run on, NULL = the library's stream */
+} vc_request;
+
+/* Result of one graph.  For MVC `size` is the minimum cover size (upper bound on
+ * VC_TIMEOUT / VC_BUDGET) and `decision` is 1; for PVC `decision` is 1 iff a
+ * cover of size <= k exists (the reference's kFound, main.cu:355-356) and
+ * `size` is the size of the cover returned.  `cover_mask` (caller-owned, n
+ * bytes, may be NULL) receives 1 for every vertex in the returned cover; when
+ * no cover of size <= ub was found (MVC with ub < OPT+... or PVC "no") it is
+ * left zeroed and has_cover is 0. */
+typedef struct vc_result {
+    uint32_t size;
+    uint32_t decision;
+    uint32_t has_cover;
+    vc_status status;
+    uint8_t *cover_mask;
+    uint64_t tree_nodes;  /* search-tree nodes whose reduction fixpoint was computed */
+    float kernel_ms;      /* device time of the search launch */
+    float total_ms;       /* wall time of the call, copies included */
+} vc_result;
+
+/* Plain one-graph solve; replaces the host path of main.cu:101-359 (device
+ * query, sizing, allocation, the GlobalWorkList / GlobalWorkListParameterized
+ * kernel launch at main.cu:302-314 and the read-back of minimum / kFound). */
+vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result *out);
+
+/* Batched solve: every graph of the arena in one persistent launch with a
+ * shared device worklist (no counterpart in the reference, which launches one
+ * graph per process).  reqs has `arena->count` entries; out likewise (each
+ * out[i].cover_mask, if non-NULL, holds n[i] bytes).  Returns the first
+ * non-OK per-graph status, or VC_OK. */
+vc_status vc_solve_batch(const vc_csr_arena *arena, const vc_request *reqs, vc_result *out);
+
+/* The same over an arena already resident on the device: `arena` holds the
+ * host copies (n, row_off, col_off, row_ptr are read on the host to size the
+ * launch), d_row_ptr / d_col the device copies the kernels read. */
+vc_status vc_solve_batch_device(const vc_csr_arena *arena, const uint32_t *d_row_ptr, const uint32_t *d_col,
+                                const vc_request *reqs, vc_result *out);
+
+/* Continuous-batching server (no counterpart in the reference).  A persistent
+ * kernel admits requests while others run; graphs and search state stay on the
+ * device.  mem_budget_bytes bounds the device arena used by admitted requests
+ * (0 = library default).  submit copies the graph and returns a ticket; poll
+ * returns VC_PENDING until the ticket's result is ready, then fills *out
+ * (out->cover_mask, if non-NULL, receives n bytes) and releases the ticket. */
+typedef struct vc_server vc_server;
+vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests, vc_server **out);
+vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket);
+vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out);
+vc_status vc_server_destroy(vc_server *s);
+
+/* Diagnostics: the kernels launched by this library since load (for checking
+ * that the device path ran), and a static status string. */
+uint64_t vc_kernel_launches(void);
+const char *vc_status_string(vc_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,75 @@
+// vc_host.h -- host-side types shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "../../include/vcgpu.h"
+#include "vc_types.h"
+
+namespace vch {
+
+// Search units are warps up to this vertex capacity, CTAs above it.
+constexpr uint32_t kWarpMaxNP = 2048;
+constexpr uint32_t kMaxVertices = 1u << 26;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
+struct PinBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+};
+
+struct Plan {
+    const void *fn = nullptr;
+    uint32_t block = 0, grid = 0, smem = 0;
+    uint32_t np = 0, su_bytes = 0, num_su = 0;
+    bool global_ws = false;
+};
+
+// Per-device state: one stream, grow-only device and pinned buffers, a lock
+// that serialises solves on the device.
+struct Ctx {
+    int dev = -1;
+    int sms = 0;
+    int smem_optin = 0;
+    int coop = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf rp, col, inst, st, covers, ctl, seq, data, gws, launches;
+    PinBuf h_st, h_desc, h_covers;
+    unsigned long long h_ctl = 0;
+    std::mutex mu;
+};
+
+struct Job {
+    const uint32_t *d_rp = nullptr;
+    const uint32_t *d_col = nullptr;
+    std::vector<vcg::InstDesc> desc;
+    double time_limit_s = 0;
+    // results
+    std::vector<vcg::InstState> st;
+    std::vector<uint32_t> covers;
+    float kernel_ms = 0;
+    bool aborted = false;
+    Plan plan;
+};
+
+Ctx *get_ctx(int dev, vc_status *err);
+cudaError_t make_plan(Ctx &c, uint32_t np, Plan &pl);
+vc_status run_job(Ctx &c, Job &job, cudaStream_t stream);
+vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out);
+vc_status validate_csr(const vc_csr *g);
+vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_result *out, const uint32_t *d_rp,
+                              const uint32_t *d_col, std::chrono::steady_clock::time_point t0);
+
+}  // namespace vch

@@ -1,0 +1,717 @@
+// vc_search.cuh -- device side of the exact MVC / PVC branch-and-reduce search.
+//
+// What it computes is the reference's search (src/GlobalWorkList.cuh:16-200 for
+// MVC, src/GlobalWorkListParameterized.cuh:13-202 for PVC): reduce a node with the
+// degree-one, degree-two/triangle and high-degree rules, prune on
+// del >= best or E >= (best-del-1)^2 + 1 (PVC: del > k or E >= (k-del)^2 + 1),
+// branch on the max-degree vertex v into "take v" and "take N(v)".  How it is
+// computed is B200-first rather than a translation:
+//
+//  * Search unit (SU) = one warp (graphs up to a few thousand vertices) or one
+//    CTA (larger graphs).  An SU owns, in shared memory: the live-degree array
+//    of its current node (int32; a deleted vertex holds a large negative value),
+//    an undo trail of the vertices deleted below its starting node, and a frame
+//    stack of pending "take N(v)" children (trail position + v).  Backtracking
+//    restores the trail instead of copying whole degree arrays (the reference
+//    copies (UB+1)*V ints per CTA, stack.cuh:10-47).
+//  * One read-only scan per reduction pass decides all three rules from the same
+//    snapshot and marks the vertices to take in a bitmap; an apply step then
+//    takes them.  The final (mark-free) scan also yields sum of degrees, max
+//    degree and its lowest-index argmax with warp redux instructions.  Taking a
+//    set of vertices chosen from one snapshot equals taking them one rule at a
+//    time (each choice stays valid or becomes a no-op after the others), so the
+//    optimum is unchanged; only the order of deletions differs from the
+//    reference's phase-by-phase loop (helperFunctions.cuh:229-447).
+//  * Work sharing: a bounded lock-free MPMC ring in global memory (L2-resident)
+//    holds donated subtrees as deleted-vertex bitmaps (n bits).  A busy SU
+//    donates its shallowest pending child only while more SUs are idle than
+//    items are queued.  Termination: one 64-bit word (pending<<32 | idle).
+//    Every spin is bounded by a deadline read from %globaltimer.
+//  * Many graphs run in one launch: SUs pull graph roots from a cursor first and
+//    the ring carries (graph id, bitmap) records, so idle SUs help whichever
+//    graph still has work.  Per-graph incumbent, token count and flags live in
+//    InstState; the graph is finished when its token count reaches zero.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vc_types.h"
+
+namespace vcg {
+// ---------------------------------------------------------------- memory ops
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// ---------------------------------------------------------------- groups
+struct WarpG {
+    static constexpr unsigned kSize = 32;
+    __device__ __forceinline__ static unsigned rank() { return threadIdx.x & 31u; }
+    __device__ __forceinline__ static void sync() { __syncwarp(); }
+    __device__ __forceinline__ static bool any(bool p) { return __any_sync(0xffffffffu, p); }
+    __device__ __forceinline__ static uint32_t sum(uint32_t x) { return __reduce_add_sync(0xffffffffu, x); }
+    __device__ __forceinline__ static uint32_t max(uint32_t x) { return __reduce_max_sync(0xffffffffu, x); }
+    __device__ __forceinline__ static uint32_t min(uint32_t x) { return __reduce_min_sync(0xffffffffu, x); }
+    __device__ __forceinline__ static uint32_t bcast(uint32_t x) { return __shfl_sync(0xffffffffu, x, 0); }
+    __device__ __forceinline__ static unsigned long long bcast64(unsigned long long x)
+    {
+        return __shfl_sync(0xffffffffu, x, 0);
+    }
+    __device__ __forceinline__ static unsigned su_local() { return threadIdx.x >> 5; }
+    __device__ __forceinline__ static unsigned su_global() { return blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); }
+    __device__ __forceinline__ static unsigned warp() { return 0; }
+    static constexpr unsigned kWarps = 1;
+};
+
+template <unsigned NT>
+struct BlockG {
+    static constexpr unsigned kSize = NT;
+    static constexpr unsigned kWarps = NT / 32;
+    __device__ __forceinline__ static unsigned rank() { return threadIdx.x; }
+    __device__ __forceinline__ static void sync() { __syncthreads(); }
+    __device__ __forceinline__ static bool any(bool p) { return __syncthreads_or(p) != 0; }
+    __device__ __forceinline__ static uint32_t reduce(uint32_t x, int op)
+    {
+        __shared__ uint32_t part[NT / 32];
+        __shared__ uint32_t res;
+        uint32_t w = op == 0 ? __reduce_add_sync(0xffffffffu, x)
+                             : (op == 1 ? __reduce_max_sync(0xffffffffu, x) : __reduce_min_sync(0xffffffffu, x));
+        if ((threadIdx.x & 31u) == 0) part[threadIdx.x >> 5] = w;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            uint32_t ident = op == 2 ? 0xffffffffu : 0u;
+            uint32_t v = threadIdx.x < NT / 32 ? part[threadIdx.x] : ident;
+            v = op == 0 ? __reduce_add_sync(0xffffffffu, v)
+                        : (op == 1 ? __reduce_max_sync(0xffffffffu, v) : __reduce_min_sync(0xffffffffu, v));
+            if (threadIdx.x == 0) res = v;
+        }
+        __syncthreads();
+        uint32_t r = res;
+        __syncthreads();
+        return r;
+    }
+    __device__ __forceinline__ static uint32_t sum(uint32_t x) { return reduce(x, 0); }
+    __device__ __forceinline__ static uint32_t max(uint32_t x) { return reduce(x, 1); }
+    __device__ __forceinline__ static uint32_t min(uint32_t x) { return reduce(x, 2); }
+    __device__ __forceinline__ static uint32_t bcast(uint32_t x)
+    {
+        __shared__ uint32_t b;
+        if (threadIdx.x == 0) b = x;
+        __syncthreads();
+        uint32_t r = b;
+        __syncthreads();
+        return r;
+    }
+    __device__ __forceinline__ static unsigned long long bcast64(unsigned long long x)
+    {
+        __shared__ unsigned long long b;
+        if (threadIdx.x == 0) b = x;
+        __syncthreads();
+        unsigned long long r = b;
+        __syncthreads();
+        return r;
+    }
+    __device__ __forceinline__ static unsigned su_local() { return 0; }
+    __device__ __forceinline__ static unsigned su_global() { return blockIdx.x; }
+    __device__ __forceinline__ static unsigned warp() { return threadIdx.x >> 5; }
+};
+
+// ---------------------------------------------------------------- SU state
+// Workspace layout (bytes), np = vertex capacity, nw = np/32:
+//   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | aux[np] (np > 65536 only)
+
+struct SU {
+    int32_t *deg;
+    uint32_t *trail, *fpos, *fv, *marks, *bits, *ctr, *aux;
+    // current graph
+    const uint32_t *rp, *cl;
+    uint32_t inst, n, nw, mode, k;
+    uint32_t base_del;
+    uint32_t fr_bot, fr_top;
+    unsigned long long local_nodes;
+    unsigned long long deadline;
+};
+
+__device__ __forceinline__ void su_bind(SU &s, uint8_t *ws, uint32_t np)
+{
+    uint32_t nw = np / 32;
+    s.deg = reinterpret_cast<int32_t *>(ws);
+    s.trail = reinterpret_cast<uint32_t *>(ws) + np;
+    s.fpos = s.trail + np;
+    s.fv = s.fpos + np;
+    s.marks = s.fv + np;
+    s.bits = s.marks + nw;
+    s.ctr = s.bits + nw;
+    s.aux = np > 65536u ? s.ctr + 4 : nullptr;
+}
+
+__device__ __forceinline__ void mark(uint32_t *marks, uint32_t v) { atomicOr(&marks[v >> 5], 1u << (v & 31u)); }
+
+__device__ __forceinline__ bool row_contains(const uint32_t *rp, const uint32_t *cl, uint32_t row, uint32_t x)
+{
+    uint32_t lo = __ldg(&rp[row]), hi = __ldg(&rp[row + 1]);
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t c = __ldg(&cl[mid]);
+        if (c == x) return true;
+        if (c < x) lo = mid + 1; else hi = mid;
+    }
+    return false;
+}
+
+// One thread takes v: claim it, log it on the trail, decrement live neighbours.
+__device__ __forceinline__ void take_one(SU &s, uint32_t v)
+{
+    int32_t old = atomicExch(&s.deg[v], kDead);
+    if (old < 0) return;
+    uint32_t idx = atomicAdd(&s.ctr[0], 1u);
+    s.trail[idx] = v;
+    volatile int32_t *dv = s.deg;
+    uint32_t e1 = __ldg(&s.rp[v + 1]);
+    for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
+        uint32_t u = __ldg(&s.cl[e]);
+        if (dv[u] >= 0) atomicSub(&s.deg[u], 1);
+    }
+}
+
+struct ScanOut {
+    uint32_t sum, maxd, amax;
+};
+
+// One reduction pass.  Returns true if marks were found and applied (another
+// pass is needed); otherwise fills `o` with the fixpoint's statistics.
+template <class G>
+__device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound, ScanOut &o)
+{
+    uint32_t sum = 0, maxd = 0, amax = kNone;
+    bool marked = false;
+    const int32_t *deg = s.deg;
+    for (uint32_t v = G::rank(); v < s.n; v += G::kSize) {
+        int32_t d = deg[v];
+        if (d <= 0) continue;
+        uint32_t ud = (uint32_t)d;
+        sum += ud;
+        if (ud > maxd) { maxd = ud; amax = v; }
+        if (ud + del >= bound) {  // high-degree rule (helperFunctions.cuh:323-327)
+            mark(s.marks, v);
+            marked = true;
+        } else if (d == 1) {      // degree-one rule (helperFunctions.cuh:252-265)
+            uint32_t e1 = __ldg(&s.rp[v + 1]);
+            for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
+                uint32_t u = __ldg(&s.cl[e]);
+                int32_t du = deg[u];
+                if (du > 0) {
+                    if (du > 1 || u < v) { mark(s.marks, u); marked = true; }
+                    break;
+                }
+            }
+        } else if (d == 2) {      // degree-two triangle rule (helperFunctions.cuh:384-417)
+            uint32_t n1 = kNone, n2 = kNone;
+            bool keep = false;
+            uint32_t e1 = __ldg(&s.rp[v + 1]);
+            for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
+                uint32_t u = __ldg(&s.cl[e]);
+                int32_t du = deg[u];
+                if (du > 0) {
+                    if (du == 1 || (du == 2 && u < v)) { keep = true; break; }
+                    if (n1 == kNone) n1 = u; else { n2 = u; break; }
+                }
+            }
+            if (!keep && n2 != kNone && row_contains(s.rp, s.cl, n2, n1)) {
+                mark(s.marks, n1);
+                mark(s.marks, n2);
+                marked = true;
+            }
+        }
+    }
+    if (G::any(marked)) {
+        G::sync();  // the vote is not a memory barrier: make every lane's marks visible
+        for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) {
+            uint32_t m = s.marks[w];
+            if (!m) continue;
+            s.marks[w] = 0;
+            while (m) {
+                uint32_t b = __ffs(m) - 1;
+                m &= m - 1;
+                take_one(s, w * 32 + b);
+            }
+        }
+        G::sync();
+        return true;
+    }
+    o.sum = G::sum(sum);
+    o.maxd = G::max(maxd);
+    o.amax = G::min((maxd == o.maxd && maxd > 0) ? amax : kNone);
+    return false;
+}
+
+// Left child: take the branching vertex v (helperFunctions.cuh:200-215).
+template <class G>
+__device__ __forceinline__ void take_vertex(SU &s, uint32_t v)
+{
+    uint32_t ok = 0;
+    if (G::rank() == 0) {
+        int32_t old = atomicExch(&s.deg[v], kDead);
+        if (old >= 0) {
+            s.trail[s.ctr[0]] = v;
+            s.ctr[0] += 1;
+            ok = 1;
+        }
+    }
+    ok = G::bcast(ok);
+    if (ok) {
+        volatile int32_t *dv = s.deg;
+        uint32_t e1 = __ldg(&s.rp[v + 1]);
+        for (uint32_t e = __ldg(&s.rp[v]) + G::rank(); e < e1; e += G::kSize) {
+            uint32_t u = __ldg(&s.cl[e]);
+            if (dv[u] >= 0) atomicSub(&s.deg[u], 1);
+        }
+    }
+    G::sync();
+}
+
+// Right child: take every live neighbour of v (helperFunctions.cuh:156-184).
+template <class G>
+__device__ __forceinline__ void take_neighbours(SU &s, uint32_t v)
+{
+    uint32_t e1 = __ldg(&s.rp[v + 1]);
+    for (uint32_t e = __ldg(&s.rp[v]) + G::rank(); e < e1; e += G::kSize) take_one(s, __ldg(&s.cl[e]));
+    G::sync();
+}
+
+// Undo the trail back to position `pos` (vertices become live again with their
+// exact live-neighbour counts).
+template <class G>
+__device__ __forceinline__ void restore_to(SU &s, uint32_t pos)
+{
+    uint32_t top = s.ctr[0];
+    for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) s.deg[s.trail[i]] = kRestoring;
+    G::sync();
+    volatile int32_t *dv = s.deg;
+    for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {
+        uint32_t v = s.trail[i];
+        uint32_t c = 0;
+        uint32_t e1 = __ldg(&s.rp[v + 1]);
+        for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
+            uint32_t u = __ldg(&s.cl[e]);
+            int32_t d = dv[u];
+            if (d == kRestoring) ++c;
+            else if (d >= 0) { atomicAdd(&s.deg[u], 1); ++c; }
+        }
+        if (s.aux) s.aux[i] = c; else s.trail[i] = v | (c << 16);
+    }
+    G::sync();
+    for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {
+        uint32_t t = s.trail[i];
+        if (s.aux) s.deg[t] = (int32_t)s.aux[i];
+        else s.deg[t & 0xffffu] = (int32_t)(t >> 16);
+    }
+    G::sync();
+    if (G::rank() == 0) s.ctr[0] = pos;
+    G::sync();
+}
+
+// bits[w] = 1 for every deleted vertex of the current state (warp ballots).
+template <class G>
+__device__ __forceinline__ void dead_bits(SU &s, uint32_t *dst)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint32_t w = G::warp(); w < s.nw; w += G::kWarps) {
+        uint32_t word = __ballot_sync(0xffffffffu, s.deg[w * 32 + lane] < 0);
+        if (lane == 0) dst[w] = word;
+    }
+}
+
+// Rebuild the degree array from a deleted-vertex bitmap in s.bits.
+template <class G>
+__device__ __forceinline__ void rebuild(SU &s)
+{
+    uint32_t pad_end = s.nw * 32;
+    for (uint32_t v = G::rank(); v < pad_end; v += G::kSize) {
+        if (v >= s.n) { s.deg[v] = 0; continue; }
+        if ((s.bits[v >> 5] >> (v & 31u)) & 1u) { s.deg[v] = kDead; continue; }
+        uint32_t c = 0;
+        uint32_t e1 = __ldg(&s.rp[v + 1]);
+        for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
+            uint32_t u = __ldg(&s.cl[e]);
+            c += ((s.bits[u >> 5] >> (u & 31u)) & 1u) ^ 1u;
+        }
+        s.deg[v] = (int32_t)c;
+    }
+    uint32_t pc = 0;
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) pc += __popc(s.bits[w]);
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
+    s.base_del = G::sum(pc);
+    if (G::rank() == 0) s.ctr[0] = 0;
+    G::sync();
+}
+
+template <class G>
+__device__ __forceinline__ void bind_graph(SU &s, const Params &P, uint32_t inst)
+{
+    const InstDesc &d = P.inst[inst];
+    s.inst = inst;
+    s.n = d.n;
+    s.nw = d.nw;
+    s.mode = d.mode;
+    s.k = d.k;
+    s.rp = P.row_ptr + d.row_off;
+    s.cl = P.col + d.col_off;
+    s.fr_bot = s.fr_top = 0;
+    s.local_nodes = 0;
+}
+
+// Root of a graph: the input degrees.
+template <class G>
+__device__ __forceinline__ void load_root(SU &s)
+{
+    uint32_t pad_end = s.nw * 32;
+    for (uint32_t v = G::rank(); v < pad_end; v += G::kSize)
+        s.deg[v] = v < s.n ? (int32_t)(__ldg(&s.rp[v + 1]) - __ldg(&s.rp[v])) : 0;
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
+    s.base_del = 0;
+    if (G::rank() == 0) s.ctr[0] = 0;
+    G::sync();
+}
+
+// ---------------------------------------------------------------- ring
+__device__ __forceinline__ bool ring_claim_enq(const Params &P, unsigned long long &pos_out)
+{
+    for (int it = 0; it < 4096; ++it) {
+        unsigned long long pos = ld_relaxed_u64(&P.ctl[kTail]);
+        unsigned long long seq = ld_acquire_u64(&P.pool_seq[pos & P.q_mask]);
+        long long dif = (long long)(seq - pos);
+        if (dif == 0) {
+            if (atomicCAS(&P.ctl[kTail], pos, pos + 1) == pos) { pos_out = pos; return true; }
+        } else if (dif < 0) {
+            return false;  // full
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool ring_claim_deq(const Params &P, unsigned long long &pos_out)
+{
+    for (int it = 0; it < 4096; ++it) {
+        unsigned long long pos = ld_relaxed_u64(&P.ctl[kHead]);
+        unsigned long long seq = ld_acquire_u64(&P.pool_seq[pos & P.q_mask]);
+        long long dif = (long long)(seq - (pos + 1));
+        if (dif == 0) {
+            if (atomicCAS(&P.ctl[kHead], pos, pos + 1) == pos) { pos_out = pos; return true; }
+        } else if (dif < 0) {
+            return false;  // empty, or the producer has not published yet
+        }
+    }
+    return false;
+}
+
+// Donate the shallowest pending child.  Returns true if it left this SU.
+template <class G>
+__device__ bool donate(SU &s, const Params &P)
+{
+    uint32_t pos = s.fpos[s.fr_bot], v = s.fv[s.fr_bot];
+    uint32_t top = s.ctr[0];
+    dead_bits<G>(s, s.bits);
+    G::sync();
+    for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {
+        uint32_t u = s.trail[i];
+        atomicAnd(&s.bits[u >> 5], ~(1u << (u & 31u)));
+    }
+    G::sync();
+    uint32_t e1 = __ldg(&s.rp[v + 1]);
+    for (uint32_t e = __ldg(&s.rp[v]) + G::rank(); e < e1; e += G::kSize) {
+        uint32_t u = __ldg(&s.cl[e]);
+        atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
+    }
+    G::sync();
+    unsigned long long qpos = 0;
+    uint32_t ok = 0;
+    if (G::rank() == 0) {
+        atomicAdd(&P.st[s.inst].act, 1u);
+        atomicAdd(&P.ctl[kState], 1ull << 32);
+        if (ring_claim_enq(P, qpos)) {
+            ok = 1;
+        } else {
+            atomicSub(&P.st[s.inst].act, 1u);
+            atomicAdd(&P.ctl[kState], 0xffffffff00000000ull);
+        }
+    }
+    ok = G::bcast(ok);
+    if (!ok) return false;
+    qpos = G::bcast64(qpos);
+    uint32_t *slot = P.pool_data + (size_t)(qpos & P.q_mask) * P.stride;
+    if (G::rank() == 0) __stcg(&slot[0], s.inst);
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) __stcg(&slot[4 + w], s.bits[w]);
+    __threadfence();
+    G::sync();
+    if (G::rank() == 0) {
+        __threadfence();
+        st_release_u64(&P.pool_seq[qpos & P.q_mask], qpos + 1);
+    }
+    s.fr_bot += 1;
+    return true;
+}
+
+// Record a cover found at a leaf (MVC improvement or PVC success).
+template <class G>
+__device__ void report_leaf(SU &s, const Params &P, uint32_t del)
+{
+    InstState &st = P.st[s.inst];
+    const InstDesc &d = P.inst[s.inst];
+    uint32_t write = 0;
+    if (G::rank() == 0) {
+        if (s.mode == kModeMVC) {
+            uint32_t old = atomicMin(&st.best, del);
+            if (del < old) {
+                // bounded lock acquisition
+                bool got = false;
+                for (int it = 0; it < (1 << 20); ++it) {
+                    if (atomicCAS(&st.lock, 0u, 1u) == 0u) { got = true; break; }
+                    __nanosleep(64);
+                }
+                if (!got) atomicOr(&st.flags, kError);
+                else if (del < ld_relaxed_u32(&st.cover_size)) write = 1;
+                else atomicExch(&st.lock, 0u);
+            }
+        } else {
+            uint32_t old = atomicOr(&st.flags, kFound);
+            if (!(old & kFound)) write = 2;
+        }
+    }
+    write = G::bcast(write);
+    if (!write) return;
+    dead_bits<G>(s, P.covers + d.cover_off);
+    __threadfence();
+    G::sync();
+    if (G::rank() == 0) {
+        st.cover_size = del;
+        if (write == 2) atomicMin(&st.best, del);
+        __threadfence();
+        if (write == 1) atomicExch(&st.lock, 0u);
+    }
+}
+
+// The SU leaves its current graph: return its token and node count.
+template <class G>
+__device__ __forceinline__ void finish_stint(SU &s, const Params &P)
+{
+    if (G::rank() == 0) {
+        InstState &st = P.st[s.inst];
+        atomicAdd(&st.nodes, s.local_nodes);
+        __threadfence();
+        uint32_t old = atomicSub(&st.act, 1u);
+        if (old == 1u) atomicOr(&st.flags, kDone);
+    }
+    s.local_nodes = 0;
+    s.inst = kNone;
+    s.fr_bot = s.fr_top = 0;
+    G::sync();
+}
+
+// Acquire work: a new graph root from the cursor, else a donated record.
+// Returns false when the launch is over.
+template <class G>
+__device__ bool acquire(SU &s, const Params &P, bool &cursor_open)
+{
+    if (cursor_open) {
+        uint32_t i = 0;
+        if (G::rank() == 0) i = (uint32_t)atomicAdd(&P.ctl[kCursor], 1ull);
+        i = G::bcast(i);
+        if (i < P.count) {
+            bind_graph<G>(s, P, i);
+            load_root<G>(s);
+            return true;
+        }
+        cursor_open = false;
+    }
+    if (G::rank() == 0) atomicAdd(&P.ctl[kState], 1ull);  // idle
+    uint32_t nap = 32;
+    for (;;) {
+        // 0 = wait, 1 = got a record, 2 = exit
+        uint32_t res = 0;
+        unsigned long long qpos = 0;
+        if (G::rank() == 0) {
+            if (ld_relaxed_u64(&P.ctl[kAbort]) || ld_relaxed_u64(&P.ctl[kFinish])) {
+                res = 2;
+            } else {
+                unsigned long long st = ld_relaxed_u64(&P.ctl[kState]);
+                if ((st >> 32) > 0) {
+                    if (ring_claim_deq(P, qpos)) {
+                        atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle-1
+                        res = 1;
+                    }
+                } else if ((uint32_t)st == P.num_su) {
+                    atomicExch(&P.ctl[kFinish], 1ull);
+                    res = 2;
+                }
+                if (res == 0 && globaltimer() > s.deadline) {
+                    atomicExch(&P.ctl[kAbort], 1ull);
+                    res = 2;
+                }
+            }
+        }
+        res = G::bcast(res);
+        if (res == 2) return false;
+        if (res == 1) {
+            qpos = G::bcast64(qpos);
+            uint32_t slot_i = (uint32_t)(qpos & P.q_mask);
+            const uint32_t *slot = P.pool_data + (size_t)slot_i * P.stride;
+            G::sync();
+            __threadfence();
+            uint32_t inst = __ldcg(&slot[0]);
+            bind_graph<G>(s, P, inst);
+            for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.bits[w] = __ldcg(&slot[4 + w]);
+            G::sync();
+            if (G::rank() == 0) {
+                __threadfence();
+                st_release_u64(&P.pool_seq[slot_i], qpos + P.q_mask + 1);
+            }
+            uint32_t fl = 0;
+            if (G::rank() == 0) fl = ld_relaxed_u32(&P.st[inst].flags);
+            fl = G::bcast(fl);
+            if (fl & (kFound | kBudget | kError)) {
+                finish_stint<G>(s, P);
+                if (G::rank() == 0) atomicAdd(&P.ctl[kState], 1ull);  // idle again
+                continue;
+            }
+            rebuild<G>(s);
+            return true;
+        }
+        if (G::rank() == 0) __nanosleep(nap);
+        nap = nap < 2048 ? nap * 2 : 2048;
+        G::sync();
+    }
+}
+
+template <class G>
+__device__ void su_main(const Params &P, uint8_t *ws)
+{
+    SU s;
+    su_bind(s, ws, P.np);
+    s.inst = kNone;
+    s.fr_bot = s.fr_top = 0;
+    s.local_nodes = 0;
+    s.deadline = globaltimer() + P.time_limit_ns;
+    if (G::rank() == 0 && P.launches) atomicAdd(P.launches, 1ull);
+    bool cursor_open = true;
+    bool have = false;
+    uint32_t ticks = 0;
+
+    for (;;) {
+        if (!have) {
+            if (s.inst != kNone && s.fr_top > s.fr_bot) {
+                s.fr_top -= 1;
+                restore_to<G>(s, s.fpos[s.fr_top]);
+                take_neighbours<G>(s, s.fv[s.fr_top]);
+                have = true;
+            } else {
+                if (s.inst != kNone) finish_stint<G>(s, P);
+                if (!acquire<G>(s, P, cursor_open)) break;
+                have = true;
+            }
+        }
+        // ---- one search-tree node
+        InstState &st = P.st[s.inst];
+        uint32_t best = 0, fl = 0;
+        unsigned long long stw = 0;
+        if (G::rank() == 0) {
+            best = ld_relaxed_u32(&st.best);
+            fl = ld_relaxed_u32(&st.flags);
+            stw = ld_relaxed_u64(&P.ctl[kState]);
+            if ((ticks & 255u) == 0u) {
+                if (ld_relaxed_u64(&P.ctl[kAbort])) fl |= kError;
+                else if (globaltimer() > s.deadline) { atomicExch(&P.ctl[kAbort], 1ull); fl |= kError; }
+            }
+        }
+        ++ticks;
+        best = G::bcast(best);
+        fl = G::bcast(fl);
+        stw = G::bcast64(stw);
+        if (fl & (kFound | kBudget | kError)) {  // abandon this graph
+            if (G::rank() == 0 && !(fl & (kFound | kBudget))) atomicOr(&st.flags, kCut);
+            s.fr_bot = s.fr_top = 0;
+            have = false;
+            continue;
+        }
+        s.local_nodes += 1;
+        if ((s.local_nodes & 1023ull) == 0ull) {
+            const InstDesc &d = P.inst[s.inst];
+            if (G::rank() == 0) {
+                unsigned long long tot = atomicAdd(&st.nodes, s.local_nodes) + s.local_nodes;
+                if (d.node_limit && tot >= d.node_limit) atomicOr(&st.flags, kBudget);
+            }
+            s.local_nodes = 0;
+        }
+        const uint32_t bound = s.mode == kModeMVC ? best : s.k + 1;
+        ScanOut o = {0u, 0u, kNone};
+        uint32_t del = s.base_del + s.ctr[0];
+        for (int pass = 0; pass < (1 << 20); ++pass) {
+            if (!reduce_pass<G>(s, del, bound, o)) break;
+            del = s.base_del + s.ctr[0];
+        }
+        del = s.base_del + s.ctr[0];
+        uint64_t edges = o.sum / 2;
+        bool prune;
+        if (s.mode == kModeMVC) {
+            uint32_t b2 = best;
+            if (G::rank() == 0) b2 = ld_relaxed_u32(&st.best);
+            b2 = G::bcast(b2);
+            prune = del >= b2;
+            if (!prune) {
+                uint64_t b = (uint64_t)(b2 - del - 1);
+                prune = edges >= b * b + 1;
+            }
+        } else {
+            prune = del > s.k;
+            if (!prune) {
+                uint64_t b = (uint64_t)(s.k - del);
+                prune = edges >= b * b + 1;
+            }
+        }
+        if (prune) { have = false; continue; }
+        if (o.maxd == 0) {
+            report_leaf<G>(s, P, del);
+            have = false;
+            continue;
+        }
+        // branch: push the N(v) child, continue with the v child
+        const uint32_t v = o.amax;
+        if (G::rank() == 0) {
+            s.fpos[s.fr_top] = s.ctr[0];
+            s.fv[s.fr_top] = v;
+        }
+        s.fr_top += 1;
+        G::sync();
+        // donate the shallowest pending child while SUs are starving
+        uint32_t idle = (uint32_t)stw, pending = (uint32_t)(stw >> 32);
+        if (idle > pending) donate<G>(s, P);
+        take_vertex<G>(s, v);
+    }
+}
+
+}  // namespace vcg

@@ -1,0 +1,507 @@
+// vc_solver.cu -- host side of libvcgpu.so: the C ABI (include/vcgpu.h), per-device
+// contexts with grow-only device buffers, graph validation, launch sizing and
+// result collection.  The search itself is vc_search.cuh.
+//
+// Replaces the host path of the reference's src/main.cu:101-359: device query
+// (:101-121), sizing (:122, auxFunctions.cpp:469-578), allocations (:219-269),
+// the kernel launch (:300-344) and the read-back (:348-359).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "vc_search.cuh"
+#include "vc_host.h"
+#include "../../include/vcgpu.h"
+
+using namespace vcg;
+
+namespace vch {
+
+std::atomic<uint64_t> g_launches{0};
+
+// ---------------------------------------------------------------- kernels
+template <class G, unsigned NT>
+__global__ void __launch_bounds__(NT) k_search(Params P)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint8_t *ws = P.gws ? P.gws + (size_t)G::su_global() * P.su_bytes : smem + (size_t)G::su_local() * P.su_bytes;
+    su_main<G>(P, ws);
+}
+
+__global__ void k_init_ring(unsigned long long *seq, uint32_t q)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < q) seq[i] = i;
+}
+
+__global__ void k_init_state(InstState *st, const InstDesc *d, uint32_t count)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        InstState s;
+        s.best = d[i].init_best;
+        s.act = 1;
+        s.flags = 0;
+        s.lock = 0;
+        s.cover_size = kNone;
+        s.pad = 0;
+        s.nodes = 0;
+        st[i] = s;
+    }
+}
+
+// ---------------------------------------------------------------- buffers
+cudaError_t DevBuf::ensure(size_t bytes)
+{
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    want = want + want / 4;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) { p = nullptr; return e; }
+    cap = want;
+    return cudaSuccess;
+}
+
+void DevBuf::release()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+cudaError_t PinBuf::ensure(size_t bytes)
+{
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 4096);
+    want = want + want / 4;
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e != cudaSuccess) { p = nullptr; return e; }
+    cap = want;
+    return cudaSuccess;
+}
+
+static std::mutex g_ctx_mu;
+static Ctx *g_ctx[64];
+
+Ctx *get_ctx(int dev, vc_status *err)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { *err = VC_ERR_NO_DEVICE; return nullptr; }
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess) { *err = VC_ERR_CUDA; return nullptr; }
+    }
+    if (dev >= ndev || dev >= 64) { *err = VC_ERR_INVALID; return nullptr; }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (!g_ctx[dev]) {
+        Ctx *c = new Ctx();
+        c->dev = dev;
+        if (cudaSetDevice(dev) != cudaSuccess) { delete c; *err = VC_ERR_CUDA; return nullptr; }
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) { delete c; *err = VC_ERR_CUDA; return nullptr; }
+        c->sms = prop.multiProcessorCount;
+        c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+        c->coop = prop.cooperativeLaunch;
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+            delete c;
+            *err = VC_ERR_CUDA;
+            return nullptr;
+        }
+        g_ctx[dev] = c;
+    }
+    if (cudaSetDevice(dev) != cudaSuccess) { *err = VC_ERR_CUDA; return nullptr; }
+    *err = VC_OK;
+    return g_ctx[dev];
+}
+
+// ---------------------------------------------------------------- sizing
+template <class G, unsigned NT>
+static cudaError_t plan_variant(Ctx &c, Plan &pl, uint32_t smem_per_block)
+{
+    auto fn = k_search<G, NT>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_per_block);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)NT, smem_per_block);
+    if (e != cudaSuccess) return e;
+    if (per_sm <= 0) return cudaErrorInvalidConfiguration;
+    pl.fn = (const void *)fn;
+    pl.block = NT;
+    pl.grid = (uint32_t)per_sm * (uint32_t)c.sms;
+    pl.smem = smem_per_block;
+    return cudaSuccess;
+}
+
+// Chooses the search-unit shape for a vertex capacity np: one warp per SU with
+// its workspace in shared memory for np <= kWarpMaxNP, else one 512-thread CTA
+// per SU, in shared memory while it fits, else in a global workspace.
+cudaError_t make_plan(Ctx &c, uint32_t np, Plan &pl)
+{
+    pl.np = np;
+    pl.su_bytes = su_workspace_bytes(np);
+    const uint32_t static_smem = 1024;  // reductions / broadcasts
+    const uint32_t budget = (uint32_t)c.smem_optin - static_smem;
+    if (np <= kWarpMaxNP) {
+        uint32_t warps = std::min<uint32_t>(8, budget / pl.su_bytes);
+        if (warps >= 1) {
+            cudaError_t e;
+            switch (warps) {
+            case 8: e = plan_variant<WarpG, 256>(c, pl, 8 * pl.su_bytes); break;
+            case 7: case 6: case 5: case 4: e = plan_variant<WarpG, 128>(c, pl, 4 * pl.su_bytes); break;
+            case 3: case 2: e = plan_variant<WarpG, 64>(c, pl, 2 * pl.su_bytes); break;
+            default: e = plan_variant<WarpG, 32>(c, pl, pl.su_bytes); break;
+            }
+            if (e != cudaSuccess) return e;
+            pl.num_su = pl.grid * (pl.block / 32);
+            pl.global_ws = false;
+            return cudaSuccess;
+        }
+    }
+    if (pl.su_bytes <= budget) {
+        cudaError_t e = plan_variant<BlockG<512>, 512>(c, pl, pl.su_bytes);
+        if (e != cudaSuccess) return e;
+        pl.global_ws = false;
+    } else {
+        cudaError_t e = plan_variant<BlockG<512>, 512>(c, pl, 0);
+        if (e != cudaSuccess) return e;
+        pl.global_ws = true;
+    }
+    pl.num_su = pl.grid;
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------- one launch
+// Runs every graph of `job` (arena already on the device) to completion and
+// copies back the per-graph state and cover bitmaps.
+vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
+{
+    const uint32_t count = (uint32_t)job.desc.size();
+    if (count == 0) return VC_OK;
+    uint32_t nmax = 0, cover_words = 0;
+    for (auto &d : job.desc) {
+        nmax = std::max(nmax, d.n);
+        d.cover_off = cover_words;
+        cover_words += d.nw;
+    }
+    uint32_t np = std::max<uint32_t>(32, (nmax + 31) / 32 * 32);
+    Plan pl;
+    if (make_plan(c, np, pl) != cudaSuccess) return VC_ERR_CUDA;
+    const uint32_t nw = np / 32;
+    const uint32_t stride = (4 + nw + 3) / 4 * 4;
+    uint32_t q = 1024;
+    while (q < 2 * pl.num_su) q <<= 1;
+    const size_t ring_cap_bytes = (size_t)512 << 20;
+    while (q > 64 && (size_t)q * stride * 4 > ring_cap_bytes) q >>= 1;
+
+    size_t gws_bytes = pl.global_ws ? (size_t)pl.num_su * pl.su_bytes : 0;
+    if (c.inst.ensure(sizeof(InstDesc) * count) || c.st.ensure(sizeof(InstState) * count) ||
+        c.covers.ensure(sizeof(uint32_t) * std::max<uint32_t>(cover_words, 1)) ||
+        c.ctl.ensure(sizeof(unsigned long long) * kCtlWords) || c.seq.ensure(sizeof(unsigned long long) * q) ||
+        c.data.ensure((size_t)q * stride * 4) || c.launches.ensure(sizeof(unsigned long long)) ||
+        (gws_bytes && c.gws.ensure(gws_bytes)))
+        return VC_ERR_NOMEM;
+    if (c.h_st.ensure(sizeof(InstState) * count) || c.h_desc.ensure(sizeof(InstDesc) * count) ||
+        c.h_covers.ensure(sizeof(uint32_t) * std::max<uint32_t>(cover_words, 1)))
+        return VC_ERR_NOMEM;
+
+    memcpy(c.h_desc.p, job.desc.data(), sizeof(InstDesc) * count);
+    cudaMemcpyAsync(c.inst.p, c.h_desc.p, sizeof(InstDesc) * count, cudaMemcpyHostToDevice, stream);
+    cudaMemsetAsync(c.covers.p, 0, sizeof(uint32_t) * std::max<uint32_t>(cover_words, 1), stream);
+    cudaMemsetAsync(c.ctl.p, 0, sizeof(unsigned long long) * kCtlWords, stream);
+    k_init_ring<<<(q + 255) / 256, 256, 0, stream>>>((unsigned long long *)c.seq.p, q);
+    k_init_state<<<(count + 255) / 256, 256, 0, stream>>>((InstState *)c.st.p, (const InstDesc *)c.inst.p, count);
+    g_launches += 2;
+
+    Params P;
+    P.row_ptr = job.d_rp;
+    P.col = job.d_col;
+    P.inst = (const InstDesc *)c.inst.p;
+    P.st = (InstState *)c.st.p;
+    P.covers = (uint32_t *)c.covers.p;
+    P.count = count;
+    P.num_su = pl.num_su;
+    P.ctl = (unsigned long long *)c.ctl.p;
+    P.pool_seq = (unsigned long long *)c.seq.p;
+    P.pool_data = (uint32_t *)c.data.p;
+    P.q_mask = q - 1;
+    P.stride = stride;
+    P.np = np;
+    P.su_bytes = pl.su_bytes;
+    P.gws = pl.global_ws ? (uint8_t *)c.gws.p : nullptr;
+    P.launches = nullptr;
+    double tl = job.time_limit_s > 0 ? job.time_limit_s : 300.0;
+    P.time_limit_ns = (unsigned long long)(tl * 1e9);
+
+    void *args[] = {&P};
+    cudaEventRecord(c.ev0, stream);
+    cudaError_t e = c.coop ? cudaLaunchCooperativeKernel(pl.fn, dim3(pl.grid), dim3(pl.block), args, pl.smem, stream)
+                           : cudaErrorNotSupported;
+    if (e != cudaSuccess) return VC_ERR_CUDA;
+    g_launches += 1;
+    cudaEventRecord(c.ev1, stream);
+    cudaMemcpyAsync(c.h_st.p, c.st.p, sizeof(InstState) * count, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(c.h_covers.p, c.covers.p, sizeof(uint32_t) * std::max<uint32_t>(cover_words, 1),
+                    cudaMemcpyDeviceToHost, stream);
+    unsigned long long abort_flag = 0;
+    cudaMemcpyAsync(&c.h_ctl, (unsigned long long *)c.ctl.p + kAbort, sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost, stream);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return VC_ERR_CUDA;
+    abort_flag = c.h_ctl;
+    cudaEventElapsedTime(&job.kernel_ms, c.ev0, c.ev1);
+    job.aborted = abort_flag != 0;
+    job.st.assign((InstState *)c.h_st.p, (InstState *)c.h_st.p + count);
+    job.covers.assign((uint32_t *)c.h_covers.p, (uint32_t *)c.h_covers.p + std::max<uint32_t>(cover_words, 1));
+    job.plan = pl;
+    return VC_OK;
+}
+
+// Fills one vc_result from the collected state of graph i.
+vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out)
+{
+    const InstDesc &d = job.desc[i];
+    const InstState &s = job.st[i];
+    vc_status st;
+    if (s.flags & kError) st = VC_ERR_INTERNAL;
+    else if (s.flags & kBudget) st = VC_BUDGET;
+    else if ((s.flags & kCut) || !(s.flags & kDone)) st = job.aborted ? VC_TIMEOUT : VC_ERR_INTERNAL;
+    else st = VC_OK;
+    out->status = st;
+    out->tree_nodes = s.nodes;
+    out->kernel_ms = job.kernel_ms;
+    bool have_cover = s.cover_size != kNone;
+    if (d.mode == kModeMVC) {
+        out->decision = 1;
+        if (s.best < d.init_best) out->size = s.best;
+        else out->size = ub ? ub : d.n;  // no cover below the bound: min(ub, OPT) = ub
+    } else {
+        out->decision = (s.flags & kFound) ? 1u : 0u;
+        out->size = out->decision ? s.cover_size : 0u;
+    }
+    out->has_cover = have_cover ? 1u : 0u;
+    if (out->cover_mask) {
+        if (have_cover) {
+            const uint32_t *w = job.covers.data() + d.cover_off;
+            for (uint32_t v = 0; v < d.n; ++v) out->cover_mask[v] = (uint8_t)((w[v >> 5] >> (v & 31u)) & 1u);
+        } else {
+            memset(out->cover_mask, 0, d.n);
+        }
+    }
+    return st;
+}
+
+}  // namespace vch
+
+// ---------------------------------------------------------------- C ABI
+using namespace vch;
+
+extern "C" const char *vc_status_string(vc_status s)
+{
+    switch (s) {
+    case VC_OK: return "ok";
+    case VC_ERR_INVALID: return "invalid argument";
+    case VC_ERR_CUDA: return "CUDA error";
+    case VC_ERR_NOMEM: return "out of device memory";
+    case VC_ERR_TOO_LARGE: return "graph too large";
+    case VC_TIMEOUT: return "time limit reached";
+    case VC_BUDGET: return "node limit reached";
+    case VC_ERR_INTERNAL: return "internal error";
+    case VC_ERR_NO_DEVICE: return "no CUDA device";
+    case VC_PENDING: return "pending";
+    }
+    return "unknown";
+}
+
+extern "C" uint64_t vc_kernel_launches(void) { return g_launches.load(); }
+
+static uint32_t init_best_for(const vc_request *r, uint32_t n)
+{
+    if (r->instance == VC_PVC) return n + 1;
+    uint32_t ub = r->ub ? std::min<uint32_t>(r->ub, n) : n;
+    return ub + 1;
+}
+
+extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result *out)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    if (!g || !req || !out) return VC_ERR_INVALID;
+    if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
+    const bool dev_in = (req->flags & VC_FLAG_DEVICE_INPUT) != 0;
+    if (!dev_in && !(req->flags & VC_FLAG_NO_VALIDATE)) {
+        vc_status v = validate_csr(g);
+        if (v != VC_OK) return v;
+    } else if (!g->row_ptr || (g->m && !g->col)) {
+        return VC_ERR_INVALID;
+    }
+    out->size = 0;
+    out->decision = 0;
+    out->has_cover = 0;
+    out->tree_nodes = 0;
+    out->kernel_ms = 0;
+    if (g->n == 0) {
+        out->status = VC_OK;
+        out->decision = 1;
+        out->has_cover = 1;
+        out->total_ms = 0;
+        return VC_OK;
+    }
+    if (g->n > kMaxVertices) return VC_ERR_TOO_LARGE;
+    vc_status err;
+    Ctx *c = get_ctx(req->device, &err);
+    if (!c) return err;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaStream_t stream = req->stream ? (cudaStream_t)req->stream : c->stream;
+
+    Job job;
+    if (dev_in) {
+        job.d_rp = g->row_ptr;
+        job.d_col = g->col;
+    } else {
+        size_t rp_b = sizeof(uint32_t) * ((size_t)g->n + 1), col_b = sizeof(uint32_t) * std::max<size_t>(2 * (size_t)g->m, 1);
+        if (c->rp.ensure(rp_b) || c->col.ensure(col_b)) return VC_ERR_NOMEM;
+        cudaMemcpyAsync(c->rp.p, g->row_ptr, rp_b, cudaMemcpyHostToDevice, stream);
+        if (g->m) cudaMemcpyAsync(c->col.p, g->col, sizeof(uint32_t) * 2 * (size_t)g->m, cudaMemcpyHostToDevice, stream);
+        job.d_rp = (const uint32_t *)c->rp.p;
+        job.d_col = (const uint32_t *)c->col.p;
+    }
+    InstDesc d;
+    d.n = g->n;
+    d.nw = (g->n + 31) / 32;
+    d.row_off = 0;
+    d.col_off = 0;
+    d.mode = req->instance == VC_PVC ? kModePVC : kModeMVC;
+    d.k = std::min<uint32_t>(req->k, g->n);
+    d.init_best = init_best_for(req, g->n);
+    d.cover_off = 0;
+    d.node_limit = req->node_limit;
+    job.desc.push_back(d);
+    job.time_limit_s = req->time_limit_s;
+    vc_status s = run_job(*c, job, stream);
+    if (s != VC_OK) { out->status = s; return s; }
+    s = fill_result(job, 0, req->instance == VC_MVC ? req->ub : 0, out);
+    out->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return s;
+}
+
+extern "C" vc_status vc_solve_batch(const vc_csr_arena *a, const vc_request *reqs, vc_result *out)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    if (!a || !reqs || !out) return VC_ERR_INVALID;
+    if (a->count == 0) return VC_OK;
+    if (!a->n || !a->row_off || !a->col_off || !a->row_ptr) return VC_ERR_INVALID;
+    const bool dev_in = (reqs[0].flags & VC_FLAG_DEVICE_INPUT) != 0;
+    for (uint32_t i = 1; i < a->count; ++i)
+        if (((reqs[i].flags & VC_FLAG_DEVICE_INPUT) != 0) != dev_in) return VC_ERR_INVALID;
+    if (dev_in) return VC_ERR_INVALID;  // per-graph sizes are read on the host: use vc_solve_batch_device
+    return vc_solve_batch_impl(a, reqs, out, nullptr, nullptr, t0);
+}
+
+namespace vch {
+vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_result *out, const uint32_t *d_rp,
+                              const uint32_t *d_col, std::chrono::steady_clock::time_point t0)
+{
+    const uint32_t count = a->count;
+    uint64_t rows = 0, cols = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (reqs[i].instance != VC_MVC && reqs[i].instance != VC_PVC) return VC_ERR_INVALID;
+        if (a->n[i] > kMaxVertices) return VC_ERR_TOO_LARGE;
+        rows = std::max<uint64_t>(rows, a->row_off[i] + a->n[i] + 1);
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t *rp = a->row_ptr + a->row_off[i];
+        cols = std::max<uint64_t>(cols, a->col_off[i] + rp[a->n[i]]);
+    }
+    if (!d_rp && !(reqs[0].flags & VC_FLAG_NO_VALIDATE)) {
+        for (uint32_t i = 0; i < count; ++i) {
+            vc_csr g;
+            g.n = a->n[i];
+            const uint32_t *rp = a->row_ptr + a->row_off[i];
+            g.m = rp[g.n] / 2;
+            g.row_ptr = rp;
+            g.col = a->col + a->col_off[i];
+            g.degree = nullptr;
+            vc_status v = validate_csr(&g);
+            if (v != VC_OK) return v;
+        }
+    }
+    vc_status err;
+    Ctx *c = get_ctx(reqs[0].device, &err);
+    if (!c) return err;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaStream_t stream = reqs[0].stream ? (cudaStream_t)reqs[0].stream : c->stream;
+    Job job;
+    if (d_rp) {
+        job.d_rp = d_rp;
+        job.d_col = d_col;
+    } else {
+        if (c->rp.ensure(sizeof(uint32_t) * rows) || c->col.ensure(sizeof(uint32_t) * std::max<uint64_t>(cols, 1)))
+            return VC_ERR_NOMEM;
+        cudaMemcpyAsync(c->rp.p, a->row_ptr, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, stream);
+        if (cols) cudaMemcpyAsync(c->col.p, a->col, sizeof(uint32_t) * cols, cudaMemcpyHostToDevice, stream);
+        job.d_rp = (const uint32_t *)c->rp.p;
+        job.d_col = (const uint32_t *)c->col.p;
+    }
+    job.desc.resize(count);
+    double tl = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        InstDesc &d = job.desc[i];
+        d.n = a->n[i];
+        d.nw = (d.n + 31) / 32;
+        d.row_off = a->row_off[i];
+        d.col_off = a->col_off[i];
+        d.mode = reqs[i].instance == VC_PVC ? kModePVC : kModeMVC;
+        d.k = std::min<uint32_t>(reqs[i].k, d.n);
+        d.init_best = init_best_for(&reqs[i], d.n);
+        d.node_limit = reqs[i].node_limit;
+        tl = std::max(tl, reqs[i].time_limit_s);
+    }
+    job.time_limit_s = tl;
+    vc_status s = run_job(*c, job, stream);
+    if (s != VC_OK) {
+        for (uint32_t i = 0; i < count; ++i) out[i].status = s;
+        return s;
+    }
+    vc_status first = VC_OK;
+    float total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    for (uint32_t i = 0; i < count; ++i) {
+        if (a->n[i] == 0) {
+            out[i].status = VC_OK;
+            out[i].size = 0;
+            out[i].decision = 1;
+            out[i].has_cover = 1;
+            out[i].tree_nodes = 0;
+            out[i].kernel_ms = job.kernel_ms;
+            out[i].total_ms = total;
+            continue;
+        }
+        vc_status si = fill_result(job, i, reqs[i].instance == VC_MVC ? reqs[i].ub : 0, &out[i]);
+        out[i].total_ms = total;
+        if (si != VC_OK && first == VC_OK) first = si;
+    }
+    return first;
+}
+}  // namespace vch
+
+// Batched solve over an arena already resident on the device: the per-graph
+// sizes and offsets stay on the host (`a` holds host arrays for n, row_off,
+// col_off and the row_ptr values), d_rp / d_col are the device copies.
+extern "C" vc_status vc_solve_batch_device(const vc_csr_arena *a, const uint32_t *d_rp, const uint32_t *d_col,
+                                           const vc_request *reqs, vc_result *out)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    if (!a || !reqs || !out || !d_rp) return VC_ERR_INVALID;
+    if (a->count == 0) return VC_OK;
+    return vc_solve_batch_impl(a, reqs, out, d_rp, d_col, t0);
+}

@@ -1,0 +1,79 @@
+// vc_types.h -- plain data shared by the search kernels and the host code.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define VC_HD __host__ __device__
+#else
+#define VC_HD
+#endif
+
+namespace vcg {
+
+
+constexpr int32_t kDead = -(1 << 30);
+constexpr int32_t kRestoring = -1;
+constexpr uint32_t kNone = 0xffffffffu;
+
+// InstState.flags
+constexpr uint32_t kFound = 1u;   // PVC: a cover of size <= k was found
+constexpr uint32_t kBudget = 2u;  // node limit reached
+constexpr uint32_t kDone = 4u;    // every token of the graph returned
+constexpr uint32_t kError = 8u;   // a bounded wait gave up
+constexpr uint32_t kCut = 16u;    // work was dropped at the launch's time limit
+
+// control words, each on its own 128-byte line (index in u64 units)
+enum : uint32_t { kHead = 0, kTail = 16, kState = 32, kCursor = 48, kAbort = 64, kFinish = 80, kCtlWords = 96 };
+
+enum : uint32_t { kModeMVC = 0, kModePVC = 1 };
+
+struct InstDesc {
+    uint32_t n, nw;            // vertices, 32-bit words of an n-bit set
+    uint64_t row_off, col_off; // offsets of this graph's row_ptr / col in the arena
+    uint32_t mode, k;          // kModeMVC / kModePVC, PVC parameter
+    uint32_t init_best;        // MVC: look for covers smaller than this
+    uint32_t cover_off;        // word offset of this graph's cover bitmap
+    uint64_t node_limit;       // 0 = none
+};
+
+struct InstState {
+    uint32_t best;        // MVC incumbent (init_best until a cover is found)
+    uint32_t act;         // outstanding work tokens (SU stints + queued records)
+    uint32_t flags;
+    uint32_t lock;        // guards the cover bitmap
+    uint32_t cover_size;  // size of the cover in the bitmap, kNone = none
+    uint32_t pad;
+    unsigned long long nodes;
+};
+
+struct Params {
+    const uint32_t *row_ptr;
+    const uint32_t *col;
+    const InstDesc *inst;
+    InstState *st;
+    uint32_t *covers;
+    uint32_t count;
+    uint32_t num_su;
+    unsigned long long *ctl;
+    unsigned long long *pool_seq;
+    uint32_t *pool_data;
+    uint32_t q_mask;
+    uint32_t stride;      // u32 words per ring slot (4 header words + nw)
+    uint32_t np;          // per-SU vertex capacity (multiple of 32)
+    uint32_t su_bytes;    // per-SU workspace bytes
+    uint8_t *gws;         // global workspace (CTA SUs on large graphs), else null
+    unsigned long long *launches; // device counter of SU starts (diagnostics)
+    unsigned long long time_limit_ns;
+};
+
+// Workspace layout (bytes), np = vertex capacity, nw = np/32:
+//   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | aux[np] (np > 65536 only)
+VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
+{
+    uint32_t nw = np / 32;
+    uint32_t b = 16u * np + 8u * nw + 16u;
+    if (np > 65536u) b += 4u * np;
+    return (b + 15u) & ~15u;
+}
+
+}  // namespace vcg

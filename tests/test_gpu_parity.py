@@ -1,0 +1,166 @@
+"""GPU parity: the CUDA search (through the C ABI) against the CPU oracle.
+
+The bar is bit-exact: the MVC size equals the oracle's optimum (the oracle is
+the restatement of the reference's Sequential(), pinned to the reference's own
+compiled solver by tests/test_oracle.py), every PVC decision equals the
+oracle's, and every returned cover is checked edge by edge and has exactly the
+reported size.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import vcgpu
+from vcgpu import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TL = 60.0  # seconds: every solve here finishes far below this
+
+
+def _check_mvc(g, r, opt):
+    assert r.status == vcgpu.VC_OK, (g.name, r)
+    assert r.size == opt, (g.name, r.size, opt)
+    assert r.cover is not None, g.name
+    assert int(r.cover.sum()) == opt, g.name
+    assert W.is_cover(g, r.cover), g.name
+
+
+def _check_pvc(g, r, k, expect):
+    assert r.status == vcgpu.VC_OK, (g.name, k, r)
+    assert r.decision == expect, (g.name, k, r.decision, expect)
+    if expect:
+        assert r.cover is not None and W.is_cover(g, r.cover) and int(r.cover.sum()) <= k
+        assert r.size == int(r.cover.sum())
+
+
+def test_config1_gnp60():
+    g = W.config1_graph()
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    opt = small["config1"]["opt"]
+    _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+    _check_pvc(g, vcgpu.solve(g, "pvc", k=opt, time_limit=TL), opt, 1)
+    _check_pvc(g, vcgpu.solve(g, "pvc", k=opt - 1, time_limit=TL), opt - 1, 0)
+
+
+def test_config2_planted_cover():
+    g = W.config2_graph()
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    opt = small["config2"]["opt"]
+    _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+    _check_pvc(g, vcgpu.solve(g, "pvc", k=opt, time_limit=TL), opt, 1)
+    _check_pvc(g, vcgpu.solve(g, "pvc", k=opt - 1, time_limit=TL), opt - 1, 0)
+
+
+def test_exhaustive_small_graphs_batched():
+    """Every graph on <= 5 vertices plus a seeded sample on 6 and 7 vertices, all
+    in one batched launch (empty graphs, isolated vertices, K2, triangles ...)."""
+    import itertools
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    graphs, opts = [], []
+    for n, mask, opt in small["exhaustive"]:
+        pairs = list(itertools.combinations(range(n), 2))
+        e = [pairs[j] for j in range(len(pairs)) if (mask >> j) & 1]
+        graphs.append(W.from_edges(n, np.asarray(e, dtype=np.int64).reshape(-1, 2), f"n{n}_m{mask}"))
+        opts.append(opt)
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    assert st == vcgpu.VC_OK
+    for g, r, opt in zip(graphs, sols, opts):
+        assert r.status == vcgpu.VC_OK and r.size == opt, (g.name, r, opt)
+        assert r.cover is not None and W.is_cover(g, r.cover) and int(r.cover.sum()) == opt, g.name
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_gnp_vs_oracle(seed):
+    rng = np.random.default_rng(1000 + seed)
+    n = int(rng.integers(10, 90))
+    d = float(rng.uniform(1.0, 8.0))
+    g = W.gnp(n, min(1.0, d / max(n - 1, 1)), 5000 + seed)
+    st, opt, _, _ = O.mvc(g)
+    assert st == O.OK
+    _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+    for k, expect in ((opt, 1), (opt - 1, 0), (opt + 3, 1), (max(opt - 5, 0), 0 if opt > 0 else 1)):
+        if k < 0:
+            continue
+        _check_pvc(g, vcgpu.solve(g, "pvc", k=k, time_limit=TL), k, expect)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_regular_vs_oracle(seed):
+    g = W.random_regular(40 + 10 * seed, 3, 77 + seed)
+    st, opt, _, _ = O.mvc(g)
+    assert st == O.OK
+    _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+    _check_pvc(g, vcgpu.solve(g, "pvc", k=opt - 1, time_limit=TL), opt - 1, 0)
+
+
+def test_ub_semantics_match_reference():
+    """`ub` is the reference's `minimum` argument: the answer is min(ub, OPT)."""
+    g = W.gnp(50, 0.12, 42)
+    st, opt, _, _ = O.mvc(g)
+    for ub in (opt + 5, opt, opt - 1, opt - 3):
+        r = vcgpu.solve(g, "mvc", ub=ub, time_limit=TL)
+        assert r.status == vcgpu.VC_OK
+        assert r.size == min(ub, opt), (ub, opt, r.size)
+        if ub >= opt:
+            assert r.cover is not None and W.is_cover(g, r.cover) and int(r.cover.sum()) == opt
+        else:
+            assert r.cover is None
+
+
+def _golden_batch(max_nodes):
+    path = os.path.join(GOLDEN, "batch_seed0.jsonl")
+    recs = [json.loads(l) for l in open(path) if l.strip()]
+    return sorted([r for r in recs if r["status"] == "ok" and r["nodes"] <= max_nodes], key=lambda r: r["i"])
+
+
+def test_batch_instances_vs_golden():
+    """A slice of the batched workload (G(n, p), n in [30, 200], average degree
+    in [3, 12]) in one launch, against the oracle's pinned optima."""
+    recs = _golden_batch(2_000_000)[:256]
+    graphs = [W.batch_instance(r["i"]) for r in recs]
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    assert st == vcgpu.VC_OK
+    for g, r, rec in zip(graphs, sols, recs):
+        _check_mvc(g, r, rec["opt"])
+
+
+def test_plain_equals_batched():
+    recs = _golden_batch(200_000)[:16]
+    graphs = [W.batch_instance(r["i"]) for r in recs]
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    for g, rb, rec in zip(graphs, sols, recs):
+        rp = vcgpu.solve(g, "mvc", time_limit=TL)
+        assert rp.size == rb.size == rec["opt"]
+
+
+def test_node_limit_reports_budget():
+    recs = [r for r in _golden_batch(10**9) if r["nodes"] > 100_000]
+    g = W.batch_instance(recs[0]["i"])
+    r = vcgpu.solve(g, "mvc", node_limit=2000, time_limit=TL)
+    assert r.status == vcgpu.VC_BUDGET
+    assert r.size >= recs[0]["opt"]
+    if r.cover is not None:
+        assert W.is_cover(g, r.cover) and int(r.cover.sum()) == r.size
+
+
+def test_invalid_graphs_rejected():
+    g = W.gnp(20, 0.2, 1)
+    bad = W.Graph(g.n, g.row_ptr.copy(), g.col.copy())
+    bad.col[0] = bad.n + 5  # id out of range
+    assert vcgpu.solve(bad).status == vcgpu.VC_ERR_INVALID
+    loop = W.Graph(3, np.array([0, 1, 2, 2], np.uint32), np.array([0, 0], np.uint32))  # self-loop
+    assert vcgpu.solve(loop).status == vcgpu.VC_ERR_INVALID
+    asym = W.Graph(3, np.array([0, 1, 1, 1], np.uint32), np.array([1], np.uint32))  # one direction only
+    assert vcgpu.solve(asym).status == vcgpu.VC_ERR_INVALID
+
+
+def test_empty_and_edgeless():
+    assert vcgpu.solve(W.from_edges(0, np.zeros((0, 2)))).size == 0
+    r = vcgpu.solve(W.from_edges(7, np.zeros((0, 2))), time_limit=TL)
+    assert r.status == vcgpu.VC_OK and r.size == 0 and not r.cover.any()
+    r = vcgpu.solve(W.from_edges(7, np.zeros((0, 2))), "pvc", k=0, time_limit=TL)
+    assert r.decision == 1
