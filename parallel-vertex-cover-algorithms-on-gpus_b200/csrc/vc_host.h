@@ -32,7 +32,7 @@ struct PinBuf {
 struct Plan {
     const void *fn = nullptr;
     uint32_t block = 0, grid = 0, smem = 0;
-    uint32_t np = 0, su_bytes = 0, num_su = 0;
+    uint32_t np = 0, su_bytes = 0, num_su = 0, stride = 0, cta_slots = 0;
     bool global_ws = false;
 };
 
@@ -48,6 +48,11 @@ struct Ctx {
     DevBuf rp, col, inst, st, covers, ctl, seq, data, gws, launches;
     PinBuf h_st, h_desc, h_covers;
     unsigned long long h_ctl = 0;
+    bool stats_on = false;
+    DevBuf stats;
+    std::vector<unsigned long long> last_stats;
+    uint32_t last_num_su = 0;
+    Plan last_plan;
     std::mutex mu;
 };
 

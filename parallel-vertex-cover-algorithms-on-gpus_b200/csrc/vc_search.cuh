@@ -145,13 +145,19 @@ struct BlockG {
 // Workspace layout (bytes), np = vertex capacity, nw = np/32:
 //   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | aux[np] (np > 65536 only)
 
+struct SUStat {
+    unsigned long long passes, donations, donate_fail, receives, roots, busy, idle, polls, restored;
+};
+
 struct SU {
+    SUStat stat;
     int32_t *deg;
     uint32_t *trail, *fpos, *fv, *marks, *bits, *ctr, *aux;
     // current graph
     const uint32_t *rp, *cl;
     uint32_t inst, n, nw, mode, k;
     uint32_t base_del;
+    uint32_t c_best;  // cached incumbent (refreshed every few nodes; stale values only weaken pruning)
     uint32_t fr_bot, fr_top;
     unsigned long long local_nodes;
     unsigned long long deadline;
@@ -249,6 +255,7 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
             }
         }
     }
+    s.stat.passes += 1;
     if (G::any(marked)) {
         G::sync();  // the vote is not a memory barrier: make every lane's marks visible
         for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) {
@@ -310,6 +317,7 @@ template <class G>
 __device__ __forceinline__ void restore_to(SU &s, uint32_t pos)
 {
     uint32_t top = s.ctr[0];
+    s.stat.restored += top - pos;
     for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) s.deg[s.trail[i]] = kRestoring;
     G::sync();
     volatile int32_t *dv = s.deg;
@@ -399,10 +407,13 @@ __device__ __forceinline__ void load_root(SU &s)
     G::sync();
 }
 
-// ---------------------------------------------------------------- ring
+// ---------------------------------------------------------------- global ring
+// Bounded MPMC ring (per-slot sequence numbers).  Both claims give up after a
+// few attempts instead of spinning: a failed claim is retried by the caller
+// after a back-off.
 __device__ __forceinline__ bool ring_claim_enq(const Params &P, unsigned long long &pos_out)
 {
-    for (int it = 0; it < 4096; ++it) {
+    for (int it = 0; it < 8; ++it) {
         unsigned long long pos = ld_relaxed_u64(&P.ctl[kTail]);
         unsigned long long seq = ld_acquire_u64(&P.pool_seq[pos & P.q_mask]);
         long long dif = (long long)(seq - pos);
@@ -417,7 +428,7 @@ __device__ __forceinline__ bool ring_claim_enq(const Params &P, unsigned long lo
 
 __device__ __forceinline__ bool ring_claim_deq(const Params &P, unsigned long long &pos_out)
 {
-    for (int it = 0; it < 4096; ++it) {
+    for (int it = 0; it < 2; ++it) {
         unsigned long long pos = ld_relaxed_u64(&P.ctl[kHead]);
         unsigned long long seq = ld_acquire_u64(&P.pool_seq[pos & P.q_mask]);
         long long dif = (long long)(seq - (pos + 1));
@@ -430,9 +441,24 @@ __device__ __forceinline__ bool ring_claim_deq(const Params &P, unsigned long lo
     return false;
 }
 
-// Donate the shallowest pending child.  Returns true if it left this SU.
+// ---------------------------------------------------------------- CTA pool
+// The warps of one CTA share work through shared memory; only fully idle CTAs
+// take work from the global ring, and only one warp per CTA polls it.
+enum : uint32_t { kCpIdle = 0, kCpCount, kCpPoller, kCpRegistered, kCpExit, kCpHdrWords = 8 };
+
+struct CtaPool {
+    uint32_t *hdr;        // kCpHdrWords control words (shared memory)
+    uint32_t *state;      // [lp] 0 empty, 1 being written, 2 full, 3 being read
+    uint32_t *data;       // [lp][stride]
+    uint32_t lp, su;      // slots, search units in this CTA
+};
+
+__device__ __forceinline__ uint32_t vld(const uint32_t *p) { return *(volatile const uint32_t *)p; }
+
+// Bitmap of the child to donate: frame state (dead now minus the trail above the
+// frame) plus N(v).  Left in s.bits.
 template <class G>
-__device__ bool donate(SU &s, const Params &P)
+__device__ __forceinline__ void donation_bits(SU &s)
 {
     uint32_t pos = s.fpos[s.fr_bot], v = s.fv[s.fr_bot];
     uint32_t top = s.ctr[0];
@@ -449,23 +475,58 @@ __device__ bool donate(SU &s, const Params &P)
         atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
     }
     G::sync();
+}
+
+// Donate the shallowest pending child to a sibling warp of this CTA.
+template <class G>
+__device__ bool donate_local(SU &s, const Params &P, CtaPool &cp)
+{
+    uint32_t slot = kNone;
+    if (G::rank() == 0) {
+        for (uint32_t i = 0; i < cp.lp; ++i)
+            if (atomicCAS(&cp.state[i], 0u, 1u) == 0u) { slot = i; break; }
+    }
+    slot = G::bcast(slot);
+    if (slot == kNone) { s.stat.donate_fail += 1; return false; }
+    donation_bits<G>(s);
+    uint32_t *d = cp.data + (size_t)slot * P.stride;
+    if (G::rank() == 0) {
+        d[0] = s.inst;
+        atomicAdd(&P.st[s.inst].act, 1u);
+    }
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) d[4 + w] = s.bits[w];
+    __threadfence_block();
+    G::sync();
+    if (G::rank() == 0) {
+        __threadfence_block();
+        atomicExch(&cp.state[slot], 2u);
+        atomicAdd(&cp.hdr[kCpCount], 1u);
+    }
+    s.fr_bot += 1;
+    s.stat.donations += 1;
+    return true;
+}
+
+// Donate the shallowest pending child to the global ring (for idle CTAs).
+template <class G>
+__device__ bool donate_global(SU &s, const Params &P)
+{
     unsigned long long qpos = 0;
     uint32_t ok = 0;
     if (G::rank() == 0) {
-        atomicAdd(&P.st[s.inst].act, 1u);
         atomicAdd(&P.ctl[kState], 1ull << 32);
-        if (ring_claim_enq(P, qpos)) {
-            ok = 1;
-        } else {
-            atomicSub(&P.st[s.inst].act, 1u);
-            atomicAdd(&P.ctl[kState], 0xffffffff00000000ull);
-        }
+        if (ring_claim_enq(P, qpos)) ok = 1;
+        else atomicAdd(&P.ctl[kState], 0xffffffff00000000ull);
     }
     ok = G::bcast(ok);
-    if (!ok) return false;
+    if (!ok) { s.stat.donate_fail += 1; return false; }
     qpos = G::bcast64(qpos);
+    donation_bits<G>(s);
     uint32_t *slot = P.pool_data + (size_t)(qpos & P.q_mask) * P.stride;
-    if (G::rank() == 0) __stcg(&slot[0], s.inst);
+    if (G::rank() == 0) {
+        atomicAdd(&P.st[s.inst].act, 1u);
+        __stcg(&slot[0], s.inst);
+    }
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) __stcg(&slot[4 + w], s.bits[w]);
     __threadfence();
     G::sync();
@@ -474,6 +535,7 @@ __device__ bool donate(SU &s, const Params &P)
         st_release_u64(&P.pool_seq[qpos & P.q_mask], qpos + 1);
     }
     s.fr_bot += 1;
+    s.stat.donations += 1;
     return true;
 }
 
@@ -488,9 +550,8 @@ __device__ void report_leaf(SU &s, const Params &P, uint32_t del)
         if (s.mode == kModeMVC) {
             uint32_t old = atomicMin(&st.best, del);
             if (del < old) {
-                // bounded lock acquisition
                 bool got = false;
-                for (int it = 0; it < (1 << 20); ++it) {
+                for (int it = 0; it < (1 << 20); ++it) {  // bounded lock acquisition
                     if (atomicCAS(&st.lock, 0u, 1u) == 0u) { got = true; break; }
                     __nanosleep(64);
                 }
@@ -498,11 +559,13 @@ __device__ void report_leaf(SU &s, const Params &P, uint32_t del)
                 else if (del < ld_relaxed_u32(&st.cover_size)) write = 1;
                 else atomicExch(&st.lock, 0u);
             }
+            s.c_best = min(old, del);
         } else {
             uint32_t old = atomicOr(&st.flags, kFound);
             if (!(old & kFound)) write = 2;
         }
     }
+    s.c_best = G::bcast(s.c_best);
     write = G::bcast(write);
     if (!write) return;
     dead_bits<G>(s, P.covers + d.cover_off);
@@ -533,10 +596,28 @@ __device__ __forceinline__ void finish_stint(SU &s, const Params &P)
     G::sync();
 }
 
-// Acquire work: a new graph root from the cursor, else a donated record.
-// Returns false when the launch is over.
+// Starts work on a received record (bits already in s.bits, graph bound);
+// returns false if its graph no longer needs work.
 template <class G>
-__device__ bool acquire(SU &s, const Params &P, bool &cursor_open)
+__device__ __forceinline__ bool start_record(SU &s, const Params &P)
+{
+    uint32_t fl = 0;
+    if (G::rank() == 0) fl = ld_relaxed_u32(&P.st[s.inst].flags);
+    fl = G::bcast(fl);
+    if (fl & (kFound | kBudget | kError)) {
+        finish_stint<G>(s, P);
+        return false;
+    }
+    rebuild<G>(s);
+    s.stat.receives += 1;
+    return true;
+}
+
+// Acquire work: a new graph root from the cursor, else a record from the CTA
+// pool, else (fully idle CTA, one poller) from the global ring.  Returns false
+// when the launch is over.
+template <class G>
+__device__ bool acquire(SU &s, const Params &P, CtaPool &cp, bool &cursor_open)
 {
     if (cursor_open) {
         uint32_t i = 0;
@@ -545,82 +626,132 @@ __device__ bool acquire(SU &s, const Params &P, bool &cursor_open)
         if (i < P.count) {
             bind_graph<G>(s, P, i);
             load_root<G>(s);
+            s.stat.roots += 1;
             return true;
         }
         cursor_open = false;
     }
-    if (G::rank() == 0) atomicAdd(&P.ctl[kState], 1ull);  // idle
-    uint32_t nap = 32;
+    if (G::rank() == 0) {
+        __threadfence_block();
+        atomicAdd(&cp.hdr[kCpIdle], 1u);
+    }
+    bool poller = false;  // meaningful in rank 0 only
+    uint32_t nap = 64;
     for (;;) {
-        // 0 = wait, 1 = got a record, 2 = exit
-        uint32_t res = 0;
+        s.stat.polls += 1;
+        // 0 wait, 1 local slot, 2 global record, 3 exit
+        uint32_t res = 0, slot = 0;
         unsigned long long qpos = 0;
         if (G::rank() == 0) {
-            if (ld_relaxed_u64(&P.ctl[kAbort]) || ld_relaxed_u64(&P.ctl[kFinish])) {
-                res = 2;
-            } else {
-                unsigned long long st = ld_relaxed_u64(&P.ctl[kState]);
-                if ((st >> 32) > 0) {
-                    if (ring_claim_deq(P, qpos)) {
-                        atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle-1
-                        res = 1;
+            if (vld(&cp.hdr[kCpExit])) {
+                res = 3;
+            } else if (vld(&cp.hdr[kCpCount]) > 0) {
+                if (poller) { atomicExch(&cp.hdr[kCpPoller], 0u); poller = false; }
+                atomicSub(&cp.hdr[kCpIdle], 1u);  // reserve before taking: the CTA never looks idle while work moves
+                __threadfence_block();
+                for (uint32_t i = 0; i < cp.lp; ++i)
+                    if (atomicCAS(&cp.state[i], 2u, 3u) == 2u) { slot = i; res = 1; break; }
+                if (res == 0) {
+                    __threadfence_block();
+                    atomicAdd(&cp.hdr[kCpIdle], 1u);
+                }
+            } else if (poller || atomicCAS(&cp.hdr[kCpPoller], 0u, 1u) == 0u) {
+                poller = true;
+                if (ld_relaxed_u64(&P.ctl[kAbort]) || ld_relaxed_u64(&P.ctl[kFinish])) {
+                    atomicExch(&cp.hdr[kCpExit], 1u);
+                    res = 3;
+                } else {
+                    unsigned long long stw = ld_relaxed_u64(&P.ctl[kState]);
+                    uint32_t cnt = vld(&cp.hdr[kCpCount]);
+                    __threadfence_block();
+                    uint32_t idl = vld(&cp.hdr[kCpIdle]);
+                    if (!vld(&cp.hdr[kCpRegistered]) && cnt == 0 && idl == cp.su) {
+                        stw = atomicAdd(&P.ctl[kState], 1ull) + 1ull;  // this CTA is idle
+                        cp.hdr[kCpRegistered] = 1u;
                     }
-                } else if ((uint32_t)st == P.num_su) {
-                    atomicExch(&P.ctl[kFinish], 1ull);
-                    res = 2;
+                    const bool reg = vld(&cp.hdr[kCpRegistered]) != 0;
+                    if ((stw >> 32) > 0 && ring_claim_deq(P, qpos)) {
+                        if (reg) {
+                            atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle CTAs-1
+                            cp.hdr[kCpRegistered] = 0u;
+                        } else {
+                            atomicAdd(&P.ctl[kState], 0xffffffff00000000ull);
+                        }
+                        atomicSub(&cp.hdr[kCpIdle], 1u);
+                        res = 2;
+                    } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0) {
+                        atomicExch(&P.ctl[kFinish], 1ull);
+                        atomicExch(&cp.hdr[kCpExit], 1u);
+                        res = 3;
+                    } else if (globaltimer() > s.deadline) {
+                        atomicExch(&P.ctl[kAbort], 1ull);
+                        atomicExch(&cp.hdr[kCpExit], 1u);
+                        res = 3;
+                    }
                 }
-                if (res == 0 && globaltimer() > s.deadline) {
-                    atomicExch(&P.ctl[kAbort], 1ull);
-                    res = 2;
-                }
+                if (res != 0) { atomicExch(&cp.hdr[kCpPoller], 0u); poller = false; }
             }
         }
         res = G::bcast(res);
-        if (res == 2) return false;
+        if (res == 3) return false;
         if (res == 1) {
+            slot = G::bcast(slot);
+            const uint32_t *d = cp.data + (size_t)slot * P.stride;
+            __threadfence_block();
+            uint32_t inst = vld(&d[0]);
+            bind_graph<G>(s, P, inst);
+            for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.bits[w] = vld(&d[4 + w]);
+            G::sync();
+            if (G::rank() == 0) {
+                atomicSub(&cp.hdr[kCpCount], 1u);
+                __threadfence_block();
+                atomicExch(&cp.state[slot], 0u);
+            }
+            if (start_record<G>(s, P)) return true;
+            if (G::rank() == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
+            continue;
+        }
+        if (res == 2) {
             qpos = G::bcast64(qpos);
             uint32_t slot_i = (uint32_t)(qpos & P.q_mask);
-            const uint32_t *slot = P.pool_data + (size_t)slot_i * P.stride;
+            const uint32_t *g = P.pool_data + (size_t)slot_i * P.stride;
             G::sync();
             __threadfence();
-            uint32_t inst = __ldcg(&slot[0]);
+            uint32_t inst = __ldcg(&g[0]);
             bind_graph<G>(s, P, inst);
-            for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.bits[w] = __ldcg(&slot[4 + w]);
+            for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.bits[w] = __ldcg(&g[4 + w]);
             G::sync();
             if (G::rank() == 0) {
                 __threadfence();
                 st_release_u64(&P.pool_seq[slot_i], qpos + P.q_mask + 1);
             }
-            uint32_t fl = 0;
-            if (G::rank() == 0) fl = ld_relaxed_u32(&P.st[inst].flags);
-            fl = G::bcast(fl);
-            if (fl & (kFound | kBudget | kError)) {
-                finish_stint<G>(s, P);
-                if (G::rank() == 0) atomicAdd(&P.ctl[kState], 1ull);  // idle again
-                continue;
-            }
-            rebuild<G>(s);
-            return true;
+            if (start_record<G>(s, P)) return true;
+            if (G::rank() == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
+            continue;
         }
-        if (G::rank() == 0) __nanosleep(nap);
-        nap = nap < 2048 ? nap * 2 : 2048;
+        if (G::rank() == 0) __nanosleep(poller ? nap : 256);
+        nap = nap < 4096 ? nap * 2 : 4096;
         G::sync();
     }
 }
 
 template <class G>
-__device__ void su_main(const Params &P, uint8_t *ws)
+__device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
 {
     SU s;
     su_bind(s, ws, P.np);
     s.inst = kNone;
     s.fr_bot = s.fr_top = 0;
     s.local_nodes = 0;
+    s.c_best = 0;
     s.deadline = globaltimer() + P.time_limit_ns;
-    if (G::rank() == 0 && P.launches) atomicAdd(P.launches, 1ull);
+    s.stat = SUStat{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long nodes_total = 0;
+    long long t_mark = clock64();
     bool cursor_open = true;
     bool have = false;
-    uint32_t ticks = 0;
+    uint32_t ticks = 0, c_flags = 0;
+    unsigned long long c_state = 0;
 
     for (;;) {
         if (!have) {
@@ -631,34 +762,43 @@ __device__ void su_main(const Params &P, uint8_t *ws)
                 have = true;
             } else {
                 if (s.inst != kNone) finish_stint<G>(s, P);
-                if (!acquire<G>(s, P, cursor_open)) break;
+                long long t0 = clock64();
+                s.stat.busy += (unsigned long long)(t0 - t_mark);
+                bool got = acquire<G>(s, P, cp, cursor_open);
+                t_mark = clock64();
+                s.stat.idle += (unsigned long long)(t_mark - t0);
+                if (!got) break;
                 have = true;
+                ticks = 0;  // refresh the cached graph state below
             }
         }
         // ---- one search-tree node
         InstState &st = P.st[s.inst];
-        uint32_t best = 0, fl = 0;
-        unsigned long long stw = 0;
-        if (G::rank() == 0) {
-            best = ld_relaxed_u32(&st.best);
-            fl = ld_relaxed_u32(&st.flags);
-            stw = ld_relaxed_u64(&P.ctl[kState]);
-            if ((ticks & 255u) == 0u) {
-                if (ld_relaxed_u64(&P.ctl[kAbort])) fl |= kError;
-                else if (globaltimer() > s.deadline) { atomicExch(&P.ctl[kAbort], 1ull); fl |= kError; }
+        if ((ticks & 7u) == 0u) {  // refresh cached incumbent, flags and ring state
+            uint32_t b = 0, f = 0;
+            unsigned long long w = 0;
+            if (G::rank() == 0) {
+                b = ld_relaxed_u32(&st.best);
+                f = ld_relaxed_u32(&st.flags);
+                w = ld_relaxed_u64(&P.ctl[kState]);
+                if ((ticks & 255u) == 0u) {
+                    if (ld_relaxed_u64(&P.ctl[kAbort])) f |= kError;
+                    else if (globaltimer() > s.deadline) { atomicExch(&P.ctl[kAbort], 1ull); f |= kError; }
+                }
             }
+            s.c_best = G::bcast(b);
+            c_flags = G::bcast(f);
+            c_state = G::bcast64(w);
         }
         ++ticks;
-        best = G::bcast(best);
-        fl = G::bcast(fl);
-        stw = G::bcast64(stw);
-        if (fl & (kFound | kBudget | kError)) {  // abandon this graph
-            if (G::rank() == 0 && !(fl & (kFound | kBudget))) atomicOr(&st.flags, kCut);
+        if (c_flags & (kFound | kBudget | kError)) {  // abandon this graph
+            if (G::rank() == 0 && !(c_flags & (kFound | kBudget))) atomicOr(&st.flags, kCut);
             s.fr_bot = s.fr_top = 0;
             have = false;
             continue;
         }
         s.local_nodes += 1;
+        nodes_total += 1;
         if ((s.local_nodes & 1023ull) == 0ull) {
             const InstDesc &d = P.inst[s.inst];
             if (G::rank() == 0) {
@@ -667,6 +807,7 @@ __device__ void su_main(const Params &P, uint8_t *ws)
             }
             s.local_nodes = 0;
         }
+        const uint32_t best = s.c_best;
         const uint32_t bound = s.mode == kModeMVC ? best : s.k + 1;
         ScanOut o = {0u, 0u, kNone};
         uint32_t del = s.base_del + s.ctr[0];
@@ -678,12 +819,9 @@ __device__ void su_main(const Params &P, uint8_t *ws)
         uint64_t edges = o.sum / 2;
         bool prune;
         if (s.mode == kModeMVC) {
-            uint32_t b2 = best;
-            if (G::rank() == 0) b2 = ld_relaxed_u32(&st.best);
-            b2 = G::bcast(b2);
-            prune = del >= b2;
+            prune = del >= best;
             if (!prune) {
-                uint64_t b = (uint64_t)(b2 - del - 1);
+                uint64_t b = (uint64_t)(best - del - 1);
                 prune = edges >= b * b + 1;
             }
         } else {
@@ -707,10 +845,33 @@ __device__ void su_main(const Params &P, uint8_t *ws)
         }
         s.fr_top += 1;
         G::sync();
-        // donate the shallowest pending child while SUs are starving
-        uint32_t idle = (uint32_t)stw, pending = (uint32_t)(stw >> 32);
-        if (idle > pending) donate<G>(s, P);
+        // share the shallowest pending child with starving siblings, else with idle CTAs
+        uint32_t want = 0;
+        if (G::rank() == 0) {
+            uint32_t li = vld(&cp.hdr[kCpIdle]), lc = vld(&cp.hdr[kCpCount]);
+            if (li > lc) want = 1;
+            else if ((uint32_t)c_state > (uint32_t)(c_state >> 32)) want = 2;
+        }
+        want = G::bcast(want);
+        if (want == 1) donate_local<G>(s, P, cp);
+        else if (want == 2 && donate_global<G>(s, P)) c_state += 1ull << 32;
         take_vertex<G>(s, v);
+    }
+    if (P.stats && G::rank() == 0) {
+        unsigned long long *o = P.stats + (size_t)G::su_global() * kStatWords;
+        uint32_t smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        o[kStNodes] = nodes_total;
+        o[kStPasses] = s.stat.passes;
+        o[kStDonations] = s.stat.donations;
+        o[kStDonateFail] = s.stat.donate_fail;
+        o[kStReceives] = s.stat.receives;
+        o[kStRoots] = s.stat.roots;
+        o[kStBusyCycles] = s.stat.busy;
+        o[kStIdleCycles] = s.stat.idle;
+        o[kStPolls] = s.stat.polls;
+        o[kStRestored] = s.stat.restored;
+        o[kStSmid] = smid;
     }
 }
 

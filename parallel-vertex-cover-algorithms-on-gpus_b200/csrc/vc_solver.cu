@@ -26,13 +26,30 @@ namespace vch {
 
 std::atomic<uint64_t> g_launches{0};
 
+// Resident threads per SM the search kernels are register-limited for
+// (1024 -> at most 64 registers per thread, 32 warps per SM).
+#ifndef VC_MIN_THREADS_PER_SM
+#define VC_MIN_THREADS_PER_SM 1024
+#endif
+
 // ---------------------------------------------------------------- kernels
 template <class G, unsigned NT>
-__global__ void __launch_bounds__(NT) k_search(Params P)
+__global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Params P)
 {
     extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint32_t cp_hdr[kCpHdrWords];
+    const uint32_t su_per_cta = NT / G::kSize;
+    CtaPool cp;
+    cp.su = su_per_cta;
+    cp.lp = P.cta_slots;
+    cp.hdr = cp_hdr;
+    cp.state = reinterpret_cast<uint32_t *>(smem + (P.gws ? 0 : (size_t)su_per_cta * P.su_bytes));
+    cp.data = cp.state + ((P.cta_slots + 3) / 4 * 4);
+    for (uint32_t i = threadIdx.x; i < kCpHdrWords; i += blockDim.x) cp_hdr[i] = 0;
+    for (uint32_t i = threadIdx.x; i < P.cta_slots; i += blockDim.x) cp.state[i] = 0;
+    __syncthreads();
     uint8_t *ws = P.gws ? P.gws + (size_t)G::su_global() * P.su_bytes : smem + (size_t)G::su_local() * P.su_bytes;
-    su_main<G>(P, ws);
+    su_main<G>(P, ws, cp);
 }
 
 __global__ void k_init_ring(unsigned long long *seq, uint32_t q)
@@ -146,23 +163,33 @@ static cudaError_t plan_variant(Ctx &c, Plan &pl, uint32_t smem_per_block)
 }
 
 // Chooses the search-unit shape for a vertex capacity np: one warp per SU with
-// its workspace in shared memory for np <= kWarpMaxNP, else one 512-thread CTA
-// per SU, in shared memory while it fits, else in a global workspace.
+// its workspace in shared memory for np <= kWarpMaxNP (up to 8 warps per CTA,
+// sharing a CTA pool of 2 slots per warp), else one 512-thread CTA per SU, in
+// shared memory while it fits, else in a global workspace.
+static uint32_t cta_pool_bytes(uint32_t slots, uint32_t stride)
+{
+    return slots ? 4u * ((slots + 3) / 4 * 4) + 4u * slots * stride : 0u;
+}
+
 cudaError_t make_plan(Ctx &c, uint32_t np, Plan &pl)
 {
     pl.np = np;
     pl.su_bytes = su_workspace_bytes(np);
-    const uint32_t static_smem = 1024;  // reductions / broadcasts
+    pl.stride = (4 + np / 32 + 3) / 4 * 4;
+    const uint32_t static_smem = 1024;  // reductions / broadcasts / CTA pool header
     const uint32_t budget = (uint32_t)c.smem_optin - static_smem;
     if (np <= kWarpMaxNP) {
-        uint32_t warps = std::min<uint32_t>(8, budget / pl.su_bytes);
-        if (warps >= 1) {
+        uint32_t warps = 8;
+        while (warps > 1 && warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget) warps >>= 1;
+        if (warps * pl.su_bytes + cta_pool_bytes(warps > 1 ? 2 * warps : 0, pl.stride) <= budget) {
+            pl.cta_slots = warps > 1 ? 2 * warps : 0;
+            uint32_t smem = warps * pl.su_bytes + cta_pool_bytes(pl.cta_slots, pl.stride);
             cudaError_t e;
             switch (warps) {
-            case 8: e = plan_variant<WarpG, 256>(c, pl, 8 * pl.su_bytes); break;
-            case 7: case 6: case 5: case 4: e = plan_variant<WarpG, 128>(c, pl, 4 * pl.su_bytes); break;
-            case 3: case 2: e = plan_variant<WarpG, 64>(c, pl, 2 * pl.su_bytes); break;
-            default: e = plan_variant<WarpG, 32>(c, pl, pl.su_bytes); break;
+            case 8: e = plan_variant<WarpG, 256>(c, pl, smem); break;
+            case 4: e = plan_variant<WarpG, 128>(c, pl, smem); break;
+            case 2: e = plan_variant<WarpG, 64>(c, pl, smem); break;
+            default: e = plan_variant<WarpG, 32>(c, pl, smem); break;
             }
             if (e != cudaSuccess) return e;
             pl.num_su = pl.grid * (pl.block / 32);
@@ -170,6 +197,7 @@ cudaError_t make_plan(Ctx &c, uint32_t np, Plan &pl)
             return cudaSuccess;
         }
     }
+    pl.cta_slots = 0;
     if (pl.su_bytes <= budget) {
         cudaError_t e = plan_variant<BlockG<512>, 512>(c, pl, pl.su_bytes);
         if (e != cudaSuccess) return e;
@@ -199,8 +227,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     uint32_t np = std::max<uint32_t>(32, (nmax + 31) / 32 * 32);
     Plan pl;
     if (make_plan(c, np, pl) != cudaSuccess) return VC_ERR_CUDA;
-    const uint32_t nw = np / 32;
-    const uint32_t stride = (4 + nw + 3) / 4 * 4;
+    const uint32_t stride = pl.stride;
     uint32_t q = 1024;
     while (q < 2 * pl.num_su) q <<= 1;
     const size_t ring_cap_bytes = (size_t)512 << 20;
@@ -240,8 +267,14 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     P.stride = stride;
     P.np = np;
     P.su_bytes = pl.su_bytes;
+    P.cta_slots = pl.cta_slots;
     P.gws = pl.global_ws ? (uint8_t *)c.gws.p : nullptr;
-    P.launches = nullptr;
+    P.stats = nullptr;
+    if (c.stats_on) {
+        if (c.stats.ensure(sizeof(unsigned long long) * kStatWords * pl.num_su)) return VC_ERR_NOMEM;
+        cudaMemsetAsync(c.stats.p, 0, sizeof(unsigned long long) * kStatWords * pl.num_su, stream);
+        P.stats = (unsigned long long *)c.stats.p;
+    }
     double tl = job.time_limit_s > 0 ? job.time_limit_s : 300.0;
     P.time_limit_ns = (unsigned long long)(tl * 1e9);
 
@@ -265,6 +298,13 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     job.st.assign((InstState *)c.h_st.p, (InstState *)c.h_st.p + count);
     job.covers.assign((uint32_t *)c.h_covers.p, (uint32_t *)c.h_covers.p + std::max<uint32_t>(cover_words, 1));
     job.plan = pl;
+    if (c.stats_on) {
+        c.last_stats.resize((size_t)kStatWords * pl.num_su);
+        cudaMemcpy(c.last_stats.data(), c.stats.p, sizeof(unsigned long long) * kStatWords * pl.num_su,
+                   cudaMemcpyDeviceToHost);
+        c.last_num_su = pl.num_su;
+    }
+    c.last_plan = pl;
     return VC_OK;
 }
 
@@ -325,6 +365,34 @@ extern "C" const char *vc_status_string(vc_status s)
 }
 
 extern "C" uint64_t vc_kernel_launches(void) { return g_launches.load(); }
+
+// Diagnostics (not part of the reference surface): enable per-search-unit
+// counters on a device, and read the last launch's counters as rows of
+// kStatWords u64 (nodes, passes, donations, failed donations, receives, roots,
+// busy cycles, idle cycles, polls, restored vertices, SM id).  Returns the
+// number of search units; copies at most max_rows rows.
+extern "C" uint32_t vc_debug_stats(int32_t device, int32_t enable, uint64_t *rows, uint32_t max_rows,
+                                   uint32_t *launch_shape)
+{
+    vc_status err;
+    Ctx *c = get_ctx(device, &err);
+    if (!c) return 0;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (enable >= 0) c->stats_on = enable != 0;
+    uint32_t nsu = c->last_num_su;
+    if (rows) {
+        uint32_t k = std::min(nsu, max_rows);
+        memcpy(rows, c->last_stats.data(), sizeof(uint64_t) * kStatWords * k);
+    }
+    if (launch_shape) {
+        launch_shape[0] = c->last_plan.grid;
+        launch_shape[1] = c->last_plan.block;
+        launch_shape[2] = c->last_plan.smem;
+        launch_shape[3] = c->last_plan.num_su;
+        launch_shape[4] = c->last_plan.np;
+    }
+    return nsu;
+}
 
 static uint32_t init_best_for(const vc_request *r, uint32_t n)
 {

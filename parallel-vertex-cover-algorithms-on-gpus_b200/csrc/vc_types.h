@@ -27,6 +27,13 @@ enum : uint32_t { kHead = 0, kTail = 16, kState = 32, kCursor = 48, kAbort = 64,
 
 enum : uint32_t { kModeMVC = 0, kModePVC = 1 };
 
+// Per-SU counters (the role of the reference's Counters.cuh phase timers and
+// NODES_PER_SM histogram), written once when an SU exits, only when enabled.
+enum : uint32_t {
+    kStNodes = 0, kStPasses, kStDonations, kStDonateFail, kStReceives, kStRoots, kStBusyCycles, kStIdleCycles,
+    kStPolls, kStRestored, kStSmid, kStatWords = 16
+};
+
 struct InstDesc {
     uint32_t n, nw;            // vertices, 32-bit words of an n-bit set
     uint64_t row_off, col_off; // offsets of this graph's row_ptr / col in the arena
@@ -61,8 +68,9 @@ struct Params {
     uint32_t stride;      // u32 words per ring slot (4 header words + nw)
     uint32_t np;          // per-SU vertex capacity (multiple of 32)
     uint32_t su_bytes;    // per-SU workspace bytes
+    uint32_t cta_slots;   // CTA pool slots (0 when a CTA holds one SU)
     uint8_t *gws;         // global workspace (CTA SUs on large graphs), else null
-    unsigned long long *launches; // device counter of SU starts (diagnostics)
+    unsigned long long *stats;    // per-SU counters (kStatWords each), null = off
     unsigned long long time_limit_ns;
 };
 

@@ -86,6 +86,9 @@ def lib():
         L.vc_solve_batch_device.restype = ctypes.c_int
         L.vc_kernel_launches.argtypes = []
         L.vc_kernel_launches.restype = ctypes.c_uint64
+        L.vc_debug_stats.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint32,
+                                     ctypes.c_void_p]
+        L.vc_debug_stats.restype = ctypes.c_uint32
         L.vc_status_string.argtypes = [ctypes.c_int]
         L.vc_status_string.restype = ctypes.c_char_p
         if hasattr(L, "vc_server_create"):
@@ -204,6 +207,21 @@ def solve_batch(arena, instances="mvc", ks: Optional[Sequence[int]] = None, ubs:
     sols = [_solution(outs[i], covers[i][:int(arena.n[i])] if covers[i] is not None else None, int(arena.n[i]))
             for i in range(count)]
     return st, sols
+
+
+STAT_NAMES = ["nodes", "passes", "donations", "donate_fail", "receives", "roots", "busy_cycles", "idle_cycles",
+              "polls", "restored", "smid"]
+
+
+def debug_stats(enable: Optional[bool] = None, device: int = -1):
+    """Enable/disable per-search-unit counters; returns (rows[num_su, 16], launch
+    shape (grid, block, smem, num_su, np)) of the last launch."""
+    L = lib()
+    shape = np.zeros(5, dtype=np.uint32)
+    nsu = L.vc_debug_stats(device, -1 if enable is None else int(enable), None, 0, shape.ctypes.data)
+    rows = np.zeros((max(nsu, 1), 16), dtype=np.uint64)
+    L.vc_debug_stats(device, -1, rows.ctypes.data, nsu, shape.ctypes.data)
+    return rows[:nsu], shape
 
 
 def kernel_launches() -> int:
