@@ -1,0 +1,630 @@
+// vc_dense.cuh -- the search for graphs of at most 255 vertices (the batched
+// workload's G(n, p) instances, n in [30, 200], and the 60-vertex case).
+//
+// Same search as vc_search.cuh (the reference's degree-one, triangle and
+// high-degree rules, the E > b^2 prune and max-degree branching), with dense
+// bitsets instead of CSR walks:
+//
+//  * a CTA works on one graph at a time: its adjacency is staged once into
+//    shared memory as one NW-word bitmap per vertex (NW = 8: 8 KB) and shared
+//    by the CTA's warps, which split the graph's search tree among themselves
+//    through the CTA pool (vc_search.cuh);
+//  * one warp is one search unit; its node state is the live-vertex set L (NW
+//    words, uniform in every lane's registers, mirrored in shared memory); a
+//    vertex taken into the cover leaves L, so del = n - |L| and the cover is
+//    the complement of L;
+//  * deg(v) = popc(adj[v] & L), kept per vertex in a byte array (0xFF =
+//    removed); lane l owns vertices l, l+32, ...  After a pass takes a set M,
+//    only the words of M are re-counted;
+//  * the triangle test of a degree-2 vertex is one bit test and the leaf
+//    rule's neighbour one find-first-set: no serial CSR row walks;
+//  * backtracking: an undo trail of removed ids (u16) and frames of (trail
+//    position, branching vertex); restoring ORs bits back into L.
+//
+// Records exchanged through the CTA pool and the global ring are live bitmaps.
+#pragma once
+#include "vc_search.cuh"
+
+namespace vcg {
+
+constexpr uint8_t kGone = 0xFFu;  // degs[] value of a removed vertex
+
+// extra CTA header words used by the dense kernel
+enum : uint32_t { kCpStaged = 5, kCpCursorClosed = 6 };
+
+template <int NW>
+struct DSU {
+    SUStat stat;
+    const uint32_t *adj;  // CTA-shared [32*NW][NW]
+    uint32_t *frames;     // [32*NW] (trail position << 16) | vertex
+    uint32_t *marks;      // [NW]
+    uint32_t *bits;       // [NW] record / scratch
+    uint32_t *lsm;        // [NW] shared-memory mirror of L
+    uint16_t *trail;      // [32*NW]
+    uint8_t *degs;        // [32*NW]
+    uint32_t L[NW];
+    const uint32_t *rp, *cl;
+    uint32_t inst, n, nw, mode, k;
+    uint32_t base_del, top;
+    uint32_t c_best;
+    uint32_t fr_bot, fr_top;
+    unsigned long long local_nodes;
+    unsigned long long deadline;
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+template <int NW>
+__device__ __forceinline__ void dsu_bind(DSU<NW> &s, uint8_t *ws, const uint32_t *adj)
+{
+    s.adj = adj;
+    s.frames = reinterpret_cast<uint32_t *>(ws);
+    s.marks = s.frames + 32 * NW;
+    s.bits = s.marks + NW;
+    s.lsm = s.bits + NW;
+    s.trail = reinterpret_cast<uint16_t *>(s.lsm + NW);
+    s.degs = reinterpret_cast<uint8_t *>(s.trail + 32 * NW);
+}
+
+template <int NW>
+__device__ __forceinline__ void load_row(const uint32_t *row, uint32_t (&r)[NW])
+{
+    if constexpr (NW % 4 == 0) {
+#pragma unroll
+        for (int w = 0; w < NW; w += 4) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(row + w);
+            r[w] = q.x; r[w + 1] = q.y; r[w + 2] = q.z; r[w + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int w = 0; w < NW; w += 2) {
+            const uint2 q = *reinterpret_cast<const uint2 *>(row + w);
+            r[w] = q.x; r[w + 1] = q.y;
+        }
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ void mirror_L(DSU<NW> &s)
+{
+    const unsigned lane = lane_id();
+#pragma unroll
+    for (int w = 0; w < NW; ++w)
+        if (lane == (unsigned)w) s.lsm[w] = s.L[w];
+    __syncwarp();
+}
+
+// Degrees of this lane's vertices from scratch (L mirrored in s.lsm).
+template <int NW>
+__device__ __forceinline__ void dense_degrees(DSU<NW> &s)
+{
+    const unsigned lane = lane_id();
+#pragma unroll 1
+    for (int k = 0; k < NW; ++k) {
+        const uint32_t v = lane + 32u * k;
+        uint8_t dv = kGone;
+        if (v < s.n && ((s.lsm[k] >> lane) & 1u)) {
+            uint32_t r[NW];
+            load_row<NW>(s.adj + v * NW, r);
+            uint32_t c = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) c += __popc(r[w] & s.L[w]);
+            dv = (uint8_t)c;
+        }
+        s.degs[v] = dv;
+    }
+    __syncwarp();
+}
+
+// Log the vertices of M on the trail (ascending) and drop them from L.
+template <int NW>
+__device__ __forceinline__ void dense_push(DSU<NW> &s, const uint32_t (&M)[NW])
+{
+    const unsigned lane = lane_id();
+    uint32_t base = s.top;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const uint32_t m = M[w];
+        if (m) {
+            if ((m >> lane) & 1u) s.trail[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)(32u * w + lane);
+            base += __popc(m);
+        }
+        s.L[w] &= ~m;
+    }
+    s.top = base;
+    mirror_L(s);
+}
+
+// Take the set M (subset of L): trail, L, and the degrees it changes.
+template <int NW>
+__device__ __forceinline__ void dense_remove(DSU<NW> &s, const uint32_t (&M)[NW])
+{
+    const unsigned lane = lane_id();
+    dense_push(s, M);
+#pragma unroll 1
+    for (int k = 0; k < NW; ++k) {
+        const uint32_t v = lane + 32u * k;
+        const uint8_t dv = s.degs[v];
+        if (dv == kGone) continue;
+        if (!((s.lsm[k] >> lane) & 1u)) { s.degs[v] = kGone; continue; }
+        if (dv == 0) continue;
+        uint32_t r[NW];
+        load_row<NW>(s.adj + v * NW, r);
+        uint32_t dec = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) dec += __popc(r[w] & M[w]);
+        if (dec) s.degs[v] = (uint8_t)(dv - dec);
+    }
+    __syncwarp();
+}
+
+// Put the trail above `pos` back into L.
+template <int NW>
+__device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
+{
+    const unsigned lane = lane_id();
+    if (lane < NW) s.bits[lane] = 0;
+    __syncwarp();
+    for (uint32_t i = pos + lane; i < s.top; i += 32) {
+        uint32_t u = s.trail[i];
+        atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s.L[w] |= s.bits[w];
+    s.stat.restored += s.top - pos;
+    s.top = pos;
+    __syncwarp();
+}
+
+// One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh).
+template <int NW>
+__device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
+{
+    const unsigned lane = lane_id();
+    uint32_t sum = 0, maxd = 0, amax = kNone;
+    bool marked = false;
+#pragma unroll 1
+    for (int k = 0; k < NW; ++k) {
+        const uint32_t v = lane + 32u * k;
+        const uint32_t dv = s.degs[v];
+        if (dv == 0 || dv == kGone) continue;
+        sum += dv;
+        if (dv > maxd) { maxd = dv; amax = v; }
+        if (dv + del >= bound) {  // high-degree rule
+            atomicOr(&s.marks[k], 1u << lane);
+            marked = true;
+        } else if (dv <= 2) {     // degree-one / degree-two triangle rules
+            uint32_t r[NW];
+            load_row<NW>(s.adj + v * NW, r);
+            uint32_t n1 = kNone, n2 = kNone;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                uint32_t x = r[w] & s.L[w];
+                if (x && n2 == kNone) {
+                    const uint32_t u = 32u * w + (__ffs(x) - 1);
+                    if (n1 == kNone) {
+                        n1 = u;
+                        x &= x - 1;
+                        if (x) n2 = 32u * w + (__ffs(x) - 1);
+                    } else {
+                        n2 = u;
+                    }
+                }
+            }
+            if (dv == 1) {
+                const uint32_t du = s.degs[n1];
+                if (du > 1 || n1 < v) {
+                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                    marked = true;
+                }
+            } else if (n2 != kNone) {
+                const uint32_t d1 = s.degs[n1], d2 = s.degs[n2];
+                const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
+                if (!keep && ((s.adj[n2 * NW + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
+                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                    atomicOr(&s.marks[n2 >> 5], 1u << (n2 & 31u));
+                    marked = true;
+                }
+            }
+        }
+    }
+    s.stat.passes += 1;
+    if (__any_sync(0xffffffffu, marked)) {
+        __syncwarp();
+        uint32_t M[NW];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) M[w] = s.marks[w];
+        __syncwarp();
+        if (lane < NW) s.marks[lane] = 0;
+        dense_remove(s, M);
+        return true;
+    }
+    o.sum = __reduce_add_sync(0xffffffffu, sum);
+    o.maxd = __reduce_max_sync(0xffffffffu, maxd);
+    o.amax = __reduce_min_sync(0xffffffffu, (maxd == o.maxd && maxd > 0) ? amax : kNone);
+    return false;
+}
+
+// ---- the overloads the shared work-sharing code (vc_search.cuh) calls
+template <class G, int NW>
+__device__ __forceinline__ void bind_graph(DSU<NW> &s, const Params &P, uint32_t inst)
+{
+    const InstDesc &d = P.inst[inst];
+    s.inst = inst;
+    s.n = d.n;
+    s.nw = d.nw;
+    s.mode = d.mode;
+    s.k = d.k;
+    s.rp = P.row_ptr + d.row_off;
+    s.cl = P.col + d.col_off;
+    s.fr_bot = s.fr_top = 0;
+    s.local_nodes = 0;
+}
+
+template <class G, int NW>
+__device__ __forceinline__ void load_root(DSU<NW> &s)
+{
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const uint32_t lo = 32u * w;
+        s.L[w] = lo + 32u <= s.n ? 0xffffffffu : (lo < s.n ? (1u << (s.n - lo)) - 1u : 0u);
+    }
+    s.top = 0;
+    s.base_del = 0;
+    if (lane_id() < NW) s.marks[lane_id()] = 0;
+    mirror_L(s);
+    dense_degrees(s);
+}
+
+// From a received live bitmap in s.bits.
+template <class G, int NW>
+__device__ __forceinline__ void rebuild(DSU<NW> &s)
+{
+    uint32_t live = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        s.L[w] = (uint32_t)w < s.nw ? s.bits[w] : 0u;
+        live += __popc(s.L[w]);
+    }
+    s.top = 0;
+    s.base_del = s.n - live;
+    if (lane_id() < NW) s.marks[lane_id()] = 0;
+    mirror_L(s);
+    dense_degrees(s);
+}
+
+// The bottom frame's pending child as a live bitmap in s.bits: L at that frame
+// (L now plus the trail above the frame) minus N(v).
+template <class G, int NW>
+__device__ __forceinline__ void donation_bits(DSU<NW> &s)
+{
+    const unsigned lane = lane_id();
+    const uint32_t f = s.frames[s.fr_bot];
+    const uint32_t pos = f >> 16, v = f & 0xffffu;
+    if (lane < NW) s.bits[lane] = s.lsm[lane];
+    __syncwarp();
+    for (uint32_t i = pos + lane; i < s.top; i += 32) {
+        uint32_t u = s.trail[i];
+        atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
+    }
+    __syncwarp();
+    if (lane < NW) s.bits[lane] &= ~s.adj[v * NW + lane];
+    __syncwarp();
+}
+
+template <class G, int NW>
+__device__ __forceinline__ void cover_bits(DSU<NW> &s, uint32_t *dst)
+{
+    const unsigned lane = lane_id();
+    if (lane < s.nw) {
+        const uint32_t lo = 32u * lane;
+        const uint32_t valid = lo + 32u <= s.n ? 0xffffffffu : (1u << (s.n - lo)) - 1u;
+        dst[lane] = ~s.lsm[lane] & valid;
+    }
+}
+
+// Stage graph `inst`'s adjacency into the CTA's bitmaps (one warp; the CTA has
+// no other active warp when this runs).
+template <int NW>
+__device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint32_t inst)
+{
+    const unsigned lane = lane_id();
+    const InstDesc &d = P.inst[inst];
+    const uint32_t *rp = P.row_ptr + d.row_off, *cl = P.col + d.col_off;
+    for (uint32_t i = lane; i < 32u * NW * NW; i += 32) adj[i] = 0;
+    __syncwarp();
+    for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
+        uint32_t *row = adj + v * NW;
+        const uint32_t e1 = __ldg(&rp[v + 1]);
+        for (uint32_t e = __ldg(&rp[v]); e < e1; ++e) {
+            const uint32_t u = __ldg(&cl[e]);
+            row[u >> 5] |= 1u << (u & 31u);
+        }
+    }
+    __threadfence_block();
+    __syncwarp();
+}
+
+// Acquire work for a dense search unit.  Local records always belong to the
+// CTA's staged graph.  Only when the whole CTA is idle may the poller switch
+// graphs: first to the next root from the cursor, then to records of any graph
+// from the global ring.  Returns false when the launch is over.
+template <int NW>
+__device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *adj)
+{
+    using G = WarpG;
+    using S = DSU<NW>;
+    const unsigned lane = lane_id();
+    if (lane == 0) {
+        __threadfence_block();
+        atomicAdd(&cp.hdr[kCpIdle], 1u);
+    }
+    bool poller = false;
+    uint32_t nap = 64;
+    for (;;) {
+        s.stat.polls += 1;
+        // 0 wait, 1 local slot, 2 global record, 3 exit, 4 new root
+        uint32_t res = 0, slot = 0;
+        unsigned long long qpos = 0;
+        if (lane == 0) {
+            if (vld(&cp.hdr[kCpExit])) {
+                res = 3;
+            } else if (vld(&cp.hdr[kCpCount]) > 0) {
+                if (poller) { atomicExch(&cp.hdr[kCpPoller], 0u); poller = false; }
+                atomicSub(&cp.hdr[kCpIdle], 1u);
+                __threadfence_block();
+                for (uint32_t i = 0; i < cp.lp; ++i)
+                    if (atomicCAS(&cp.state[i], 2u, 3u) == 2u) { slot = i; res = 1; break; }
+                if (res == 0) {
+                    __threadfence_block();
+                    atomicAdd(&cp.hdr[kCpIdle], 1u);
+                }
+            } else if (poller || atomicCAS(&cp.hdr[kCpPoller], 0u, 1u) == 0u) {
+                poller = true;
+                const uint32_t cnt = vld(&cp.hdr[kCpCount]);
+                __threadfence_block();
+                const bool cta_idle = cnt == 0 && vld(&cp.hdr[kCpIdle]) == cp.su;
+                if (ld_relaxed_u64(&P.ctl[kAbort]) || ld_relaxed_u64(&P.ctl[kFinish])) {
+                    atomicExch(&cp.hdr[kCpExit], 1u);
+                    res = 3;
+                } else if (cta_idle && !vld(&cp.hdr[kCpCursorClosed])) {
+                    uint32_t i = (uint32_t)atomicAdd(&P.ctl[kCursor], 1ull);
+                    if (i < P.count) {
+                        atomicSub(&cp.hdr[kCpIdle], 1u);
+                        slot = i;
+                        res = 4;
+                    } else {
+                        cp.hdr[kCpCursorClosed] = 1u;
+                    }
+                }
+                if (res == 0 && vld(&cp.hdr[kCpCursorClosed])) {
+                    unsigned long long stw = ld_relaxed_u64(&P.ctl[kState]);
+                    if (!vld(&cp.hdr[kCpRegistered]) && cta_idle) {
+                        stw = atomicAdd(&P.ctl[kState], 1ull) + 1ull;
+                        cp.hdr[kCpRegistered] = 1u;
+                    }
+                    const bool reg = vld(&cp.hdr[kCpRegistered]) != 0;
+                    // a registered CTA is fully idle, so the poller may switch graphs
+                    if (reg && (stw >> 32) > 0 && ring_claim_deq(P, qpos)) {
+                        atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle CTAs-1
+                        cp.hdr[kCpRegistered] = 0u;
+                        atomicSub(&cp.hdr[kCpIdle], 1u);
+                        res = 2;
+                    } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0) {
+                        atomicExch(&P.ctl[kFinish], 1ull);
+                        atomicExch(&cp.hdr[kCpExit], 1u);
+                        res = 3;
+                    } else if (globaltimer() > s.deadline) {
+                        atomicExch(&P.ctl[kAbort], 1ull);
+                        atomicExch(&cp.hdr[kCpExit], 1u);
+                        res = 3;
+                    }
+                }
+                if (res != 0) { atomicExch(&cp.hdr[kCpPoller], 0u); poller = false; }
+            }
+        }
+        res = G::bcast(res);
+        if (res == 3) return false;
+        if (res == 4) {  // a new graph root for the whole CTA
+            slot = G::bcast(slot);
+            if (vld(&cp.hdr[kCpStaged]) != slot) {
+                stage_graph<NW>(adj, P, slot);
+                if (lane == 0) cp.hdr[kCpStaged] = slot;
+            }
+            bind_graph<G>(s, P, slot);
+            load_root<G>(s);
+            s.stat.roots += 1;
+            return true;
+        }
+        if (res == 1) {
+            slot = G::bcast(slot);
+            const uint32_t *d = cp.data + (size_t)slot * P.stride;
+            __threadfence_block();
+            const uint32_t inst = vld(&d[0]);
+            bind_graph<G>(s, P, inst);
+            for (uint32_t w = lane; w < s.nw; w += 32) s.bits[w] = vld(&d[4 + w]);
+            __syncwarp();
+            if (lane == 0) {
+                atomicSub(&cp.hdr[kCpCount], 1u);
+                __threadfence_block();
+                atomicExch(&cp.state[slot], 0u);
+            }
+            if (start_record<G, S>(s, P)) return true;
+            if (lane == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
+            continue;
+        }
+        if (res == 2) {
+            qpos = G::bcast64(qpos);
+            const uint32_t slot_i = (uint32_t)(qpos & P.q_mask);
+            const uint32_t *g = P.pool_data + (size_t)slot_i * P.stride;
+            __syncwarp();
+            __threadfence();
+            const uint32_t inst = __ldcg(&g[0]);
+            if (vld(&cp.hdr[kCpStaged]) != inst) {
+                stage_graph<NW>(adj, P, inst);
+                if (lane == 0) cp.hdr[kCpStaged] = inst;
+            }
+            bind_graph<G>(s, P, inst);
+            for (uint32_t w = lane; w < s.nw; w += 32) s.bits[w] = __ldcg(&g[4 + w]);
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence();
+                st_release_u64(&P.pool_seq[slot_i], qpos + P.q_mask + 1);
+            }
+            if (start_record<G, S>(s, P)) return true;
+            if (lane == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
+            continue;
+        }
+        if (lane == 0) __nanosleep(poller ? nap : 256);
+        nap = nap < 4096 ? nap * 2 : 4096;
+        __syncwarp();
+    }
+}
+
+template <int NW>
+__device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPool &cp)
+{
+    using G = WarpG;
+    using S = DSU<NW>;
+    S s;
+    dsu_bind(s, ws, adj);
+    s.inst = kNone;
+    s.fr_bot = s.fr_top = 0;
+    s.local_nodes = 0;
+    s.c_best = 0;
+    s.top = 0;
+    s.deadline = globaltimer() + P.time_limit_ns;
+    s.stat = SUStat{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long nodes_total = 0;
+    long long t_mark = clock64();
+    bool have = false;
+    uint32_t ticks = 0, c_flags = 0;
+    unsigned long long c_state = 0;
+    const unsigned lane = lane_id();
+
+    for (;;) {
+        if (!have) {
+            if (s.inst != kNone && s.fr_top > s.fr_bot) {
+                s.fr_top -= 1;
+                const uint32_t f = s.frames[s.fr_top];
+                const uint32_t v = f & 0xffffu;
+                dense_restore(s, f >> 16);
+                uint32_t N[NW];
+                load_row<NW>(s.adj + v * NW, N);
+#pragma unroll
+                for (int w = 0; w < NW; ++w) N[w] &= s.L[w];
+                dense_push(s, N);
+                dense_degrees(s);
+                have = true;
+            } else {
+                if (s.inst != kNone) finish_stint<G, S>(s, P);
+                long long t0 = clock64();
+                s.stat.busy += (unsigned long long)(t0 - t_mark);
+                bool got = acquire_cta<NW>(s, P, cp, adj);
+                t_mark = clock64();
+                s.stat.idle += (unsigned long long)(t_mark - t0);
+                if (!got) break;
+                have = true;
+                ticks = 0;
+            }
+        }
+        InstState &st = P.st[s.inst];
+        if ((ticks & 7u) == 0u) {
+            uint32_t b = 0, f = 0;
+            unsigned long long w = 0;
+            if (lane == 0) {
+                b = ld_relaxed_u32(&st.best);
+                f = ld_relaxed_u32(&st.flags);
+                w = ld_relaxed_u64(&P.ctl[kState]);
+                if ((ticks & 255u) == 0u) {
+                    if (ld_relaxed_u64(&P.ctl[kAbort])) f |= kError;
+                    else if (globaltimer() > s.deadline) { atomicExch(&P.ctl[kAbort], 1ull); f |= kError; }
+                }
+            }
+            s.c_best = G::bcast(b);
+            c_flags = G::bcast(f);
+            c_state = G::bcast64(w);
+        }
+        ++ticks;
+        if (c_flags & (kFound | kBudget | kError)) {
+            if (lane == 0 && !(c_flags & (kFound | kBudget))) atomicOr(&st.flags, kCut);
+            s.fr_bot = s.fr_top = 0;
+            have = false;
+            continue;
+        }
+        s.local_nodes += 1;
+        nodes_total += 1;
+        if ((s.local_nodes & 1023ull) == 0ull) {
+            const InstDesc &d = P.inst[s.inst];
+            if (lane == 0) {
+                unsigned long long tot = atomicAdd(&st.nodes, s.local_nodes) + s.local_nodes;
+                if (d.node_limit && tot >= d.node_limit) atomicOr(&st.flags, kBudget);
+            }
+            s.local_nodes = 0;
+        }
+        const uint32_t best = s.c_best;
+        const uint32_t bound = s.mode == kModeMVC ? best : s.k + 1;
+        ScanOut o = {0u, 0u, kNone};
+#pragma unroll 1
+        for (int pass = 0; pass < 4 * 32 * NW; ++pass)
+            if (!dense_pass(s, s.base_del + s.top, bound, o)) break;
+        const uint32_t del = s.base_del + s.top;
+        const uint64_t edges = o.sum / 2;
+        bool prune;
+        if (s.mode == kModeMVC) {
+            prune = del >= best;
+            if (!prune) {
+                uint64_t b = (uint64_t)(best - del - 1);
+                prune = edges >= b * b + 1;
+            }
+        } else {
+            prune = del > s.k;
+            if (!prune) {
+                uint64_t b = (uint64_t)(s.k - del);
+                prune = edges >= b * b + 1;
+            }
+        }
+        if (prune) { have = false; continue; }
+        if (o.maxd == 0) {
+            report_leaf<G, S>(s, P, del);
+            have = false;
+            continue;
+        }
+        const uint32_t v = o.amax;
+        if (lane == 0) s.frames[s.fr_top] = (s.top << 16) | v;
+        s.fr_top += 1;
+        __syncwarp();
+        uint32_t want = 0;
+        if (lane == 0) {
+            uint32_t li = vld(&cp.hdr[kCpIdle]), lc = vld(&cp.hdr[kCpCount]);
+            if (li > lc) want = 1;
+            else if ((uint32_t)c_state > (uint32_t)(c_state >> 32)) want = 2;
+        }
+        want = G::bcast(want);
+        if (want == 1) donate_local<G, S>(s, P, cp);
+        else if (want == 2 && donate_global<G, S>(s, P)) c_state += 1ull << 32;
+        uint32_t M[NW];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) M[w] = ((uint32_t)w == (v >> 5)) ? (1u << (v & 31u)) : 0u;
+        dense_remove(s, M);
+    }
+    if (P.stats && lane == 0) {
+        unsigned long long *o = P.stats + (size_t)G::su_global() * kStatWords;
+        uint32_t smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        o[kStNodes] = nodes_total;
+        o[kStPasses] = s.stat.passes;
+        o[kStDonations] = s.stat.donations;
+        o[kStDonateFail] = s.stat.donate_fail;
+        o[kStReceives] = s.stat.receives;
+        o[kStRoots] = s.stat.roots;
+        o[kStBusyCycles] = s.stat.busy;
+        o[kStIdleCycles] = s.stat.idle;
+        o[kStPolls] = s.stat.polls;
+        o[kStRestored] = s.stat.restored;
+        o[kStSmid] = smid;
+    }
+}
+
+}  // namespace vcg

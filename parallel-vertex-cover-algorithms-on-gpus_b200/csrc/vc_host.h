@@ -34,6 +34,7 @@ struct Plan {
     uint32_t block = 0, grid = 0, smem = 0;
     uint32_t np = 0, su_bytes = 0, num_su = 0, stride = 0, cta_slots = 0;
     bool global_ws = false;
+    bool dense = false;
 };
 
 // Per-device state: one stream, grow-only device and pinned buffers, a lock
@@ -49,6 +50,7 @@ struct Ctx {
     PinBuf h_st, h_desc, h_covers;
     unsigned long long h_ctl = 0;
     bool stats_on = false;
+    bool force_sparse = false;
     DevBuf stats;
     std::vector<unsigned long long> last_stats;
     uint32_t last_num_su = 0;
@@ -70,7 +72,7 @@ struct Job {
 };
 
 Ctx *get_ctx(int dev, vc_status *err);
-cudaError_t make_plan(Ctx &c, uint32_t np, Plan &pl);
+cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl);
 vc_status run_job(Ctx &c, Job &job, cudaStream_t stream);
 vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out);
 vc_status validate_csr(const vc_csr *g);

@@ -355,6 +355,9 @@ __device__ __forceinline__ void dead_bits(SU &s, uint32_t *dst)
     }
 }
 
+template <class G>
+__device__ __forceinline__ void cover_bits(SU &s, uint32_t *dst) { dead_bits<G>(s, dst); }
+
 // Rebuild the degree array from a deleted-vertex bitmap in s.bits.
 template <class G>
 __device__ __forceinline__ void rebuild(SU &s)
@@ -478,8 +481,8 @@ __device__ __forceinline__ void donation_bits(SU &s)
 }
 
 // Donate the shallowest pending child to a sibling warp of this CTA.
-template <class G>
-__device__ bool donate_local(SU &s, const Params &P, CtaPool &cp)
+template <class G, class S>
+__device__ bool donate_local(S &s, const Params &P, CtaPool &cp)
 {
     uint32_t slot = kNone;
     if (G::rank() == 0) {
@@ -508,8 +511,8 @@ __device__ bool donate_local(SU &s, const Params &P, CtaPool &cp)
 }
 
 // Donate the shallowest pending child to the global ring (for idle CTAs).
-template <class G>
-__device__ bool donate_global(SU &s, const Params &P)
+template <class G, class S>
+__device__ bool donate_global(S &s, const Params &P)
 {
     unsigned long long qpos = 0;
     uint32_t ok = 0;
@@ -540,8 +543,8 @@ __device__ bool donate_global(SU &s, const Params &P)
 }
 
 // Record a cover found at a leaf (MVC improvement or PVC success).
-template <class G>
-__device__ void report_leaf(SU &s, const Params &P, uint32_t del)
+template <class G, class S>
+__device__ void report_leaf(S &s, const Params &P, uint32_t del)
 {
     InstState &st = P.st[s.inst];
     const InstDesc &d = P.inst[s.inst];
@@ -568,7 +571,7 @@ __device__ void report_leaf(SU &s, const Params &P, uint32_t del)
     s.c_best = G::bcast(s.c_best);
     write = G::bcast(write);
     if (!write) return;
-    dead_bits<G>(s, P.covers + d.cover_off);
+    cover_bits<G>(s, P.covers + d.cover_off);
     __threadfence();
     G::sync();
     if (G::rank() == 0) {
@@ -580,8 +583,8 @@ __device__ void report_leaf(SU &s, const Params &P, uint32_t del)
 }
 
 // The SU leaves its current graph: return its token and node count.
-template <class G>
-__device__ __forceinline__ void finish_stint(SU &s, const Params &P)
+template <class G, class S>
+__device__ __forceinline__ void finish_stint(S &s, const Params &P)
 {
     if (G::rank() == 0) {
         InstState &st = P.st[s.inst];
@@ -598,14 +601,14 @@ __device__ __forceinline__ void finish_stint(SU &s, const Params &P)
 
 // Starts work on a received record (bits already in s.bits, graph bound);
 // returns false if its graph no longer needs work.
-template <class G>
-__device__ __forceinline__ bool start_record(SU &s, const Params &P)
+template <class G, class S>
+__device__ __forceinline__ bool start_record(S &s, const Params &P)
 {
     uint32_t fl = 0;
     if (G::rank() == 0) fl = ld_relaxed_u32(&P.st[s.inst].flags);
     fl = G::bcast(fl);
     if (fl & (kFound | kBudget | kError)) {
-        finish_stint<G>(s, P);
+        finish_stint<G, S>(s, P);
         return false;
     }
     rebuild<G>(s);
@@ -616,8 +619,8 @@ __device__ __forceinline__ bool start_record(SU &s, const Params &P)
 // Acquire work: a new graph root from the cursor, else a record from the CTA
 // pool, else (fully idle CTA, one poller) from the global ring.  Returns false
 // when the launch is over.
-template <class G>
-__device__ bool acquire(SU &s, const Params &P, CtaPool &cp, bool &cursor_open)
+template <class G, class S>
+__device__ bool acquire(S &s, const Params &P, CtaPool &cp, bool &cursor_open)
 {
     if (cursor_open) {
         uint32_t i = 0;
@@ -707,7 +710,7 @@ __device__ bool acquire(SU &s, const Params &P, CtaPool &cp, bool &cursor_open)
                 __threadfence_block();
                 atomicExch(&cp.state[slot], 0u);
             }
-            if (start_record<G>(s, P)) return true;
+            if (start_record<G, S>(s, P)) return true;
             if (G::rank() == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
             continue;
         }
@@ -725,7 +728,7 @@ __device__ bool acquire(SU &s, const Params &P, CtaPool &cp, bool &cursor_open)
                 __threadfence();
                 st_release_u64(&P.pool_seq[slot_i], qpos + P.q_mask + 1);
             }
-            if (start_record<G>(s, P)) return true;
+            if (start_record<G, S>(s, P)) return true;
             if (G::rank() == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
             continue;
         }
@@ -761,10 +764,10 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
                 take_neighbours<G>(s, s.fv[s.fr_top]);
                 have = true;
             } else {
-                if (s.inst != kNone) finish_stint<G>(s, P);
+                if (s.inst != kNone) finish_stint<G, SU>(s, P);
                 long long t0 = clock64();
                 s.stat.busy += (unsigned long long)(t0 - t_mark);
-                bool got = acquire<G>(s, P, cp, cursor_open);
+                bool got = acquire<G, SU>(s, P, cp, cursor_open);
                 t_mark = clock64();
                 s.stat.idle += (unsigned long long)(t_mark - t0);
                 if (!got) break;
@@ -833,7 +836,7 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
         }
         if (prune) { have = false; continue; }
         if (o.maxd == 0) {
-            report_leaf<G>(s, P, del);
+            report_leaf<G, SU>(s, P, del);
             have = false;
             continue;
         }
@@ -853,8 +856,8 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
             else if ((uint32_t)c_state > (uint32_t)(c_state >> 32)) want = 2;
         }
         want = G::bcast(want);
-        if (want == 1) donate_local<G>(s, P, cp);
-        else if (want == 2 && donate_global<G>(s, P)) c_state += 1ull << 32;
+        if (want == 1) donate_local<G, SU>(s, P, cp);
+        else if (want == 2 && donate_global<G, SU>(s, P)) c_state += 1ull << 32;
         take_vertex<G>(s, v);
     }
     if (P.stats && G::rank() == 0) {

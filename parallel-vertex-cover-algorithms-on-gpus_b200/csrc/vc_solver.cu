@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "vc_search.cuh"
+#include "vc_dense.cuh"
 #include "vc_host.h"
 #include "../../include/vcgpu.h"
 
@@ -50,6 +51,35 @@ __global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Param
     __syncthreads();
     uint8_t *ws = P.gws ? P.gws + (size_t)G::su_global() * P.su_bytes : smem + (size_t)G::su_local() * P.su_bytes;
     su_main<G>(P, ws, cp);
+}
+
+// Register budget of the dense search units (resident threads per SM).
+#ifndef VC_DENSE8_THREADS
+#define VC_DENSE8_THREADS 1024
+#endif
+template <int NW>
+struct DenseOcc {
+    static constexpr unsigned kThreads = NW >= 8 ? VC_DENSE8_THREADS : 1024;
+};
+
+template <int NW, unsigned NT>
+__global__ void __launch_bounds__(NT, DenseOcc<NW>::kThreads / NT) k_dense(Params P)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint32_t cp_hdr[kCpHdrWords];
+    const uint32_t su_per_cta = NT / 32;
+    uint32_t *adj = reinterpret_cast<uint32_t *>(smem);
+    uint8_t *ws0 = smem + dense_adj_bytes(NW);
+    CtaPool cp;
+    cp.su = su_per_cta;
+    cp.lp = P.cta_slots;
+    cp.hdr = cp_hdr;
+    cp.state = reinterpret_cast<uint32_t *>(ws0 + (size_t)su_per_cta * P.su_bytes);
+    cp.data = cp.state + ((P.cta_slots + 3) / 4 * 4);
+    for (uint32_t i = threadIdx.x; i < kCpHdrWords; i += blockDim.x) cp_hdr[i] = (i == kCpStaged) ? kNone : 0u;
+    for (uint32_t i = threadIdx.x; i < P.cta_slots; i += blockDim.x) cp.state[i] = 0;
+    __syncthreads();
+    su_main_dense<NW>(P, ws0 + (size_t)WarpG::su_local() * P.su_bytes, adj, cp);
 }
 
 __global__ void k_init_ring(unsigned long long *seq, uint32_t q)
@@ -162,17 +192,65 @@ static cudaError_t plan_variant(Ctx &c, Plan &pl, uint32_t smem_per_block)
     return cudaSuccess;
 }
 
-// Chooses the search-unit shape for a vertex capacity np: one warp per SU with
-// its workspace in shared memory for np <= kWarpMaxNP (up to 8 warps per CTA,
-// sharing a CTA pool of 2 slots per warp), else one 512-thread CTA per SU, in
-// shared memory while it fits, else in a global workspace.
 static uint32_t cta_pool_bytes(uint32_t slots, uint32_t stride)
 {
     return slots ? 4u * ((slots + 3) / 4 * 4) + 4u * slots * stride : 0u;
 }
 
-cudaError_t make_plan(Ctx &c, uint32_t np, Plan &pl)
+template <unsigned NT, class F>
+static cudaError_t plan_variant_fn(Ctx &c, Plan &pl, uint32_t smem_per_block, F fn)
 {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_per_block);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)NT, smem_per_block);
+    if (e != cudaSuccess) return e;
+    if (per_sm <= 0) return cudaErrorInvalidConfiguration;
+    pl.fn = (const void *)fn;
+    pl.block = NT;
+    pl.grid = (uint32_t)per_sm * (uint32_t)c.sms;
+    pl.smem = smem_per_block;
+    return cudaSuccess;
+}
+
+// Chooses the search-unit shape for a vertex capacity np: one warp per SU with
+// its workspace in shared memory for np <= kWarpMaxNP (up to 8 warps per CTA,
+// sharing a CTA pool of 2 slots per warp), else one 512-thread CTA per SU, in
+// shared memory while it fits, else in a global workspace.
+
+template <int NW>
+static cudaError_t plan_dense(Ctx &c, Plan &pl)
+{
+    pl.np = 32 * NW;
+    pl.su_bytes = dense_workspace_bytes(NW);
+    pl.stride = (4 + NW + 3) / 4 * 4;
+    const uint32_t budget = (uint32_t)c.smem_optin - 1024;
+    uint32_t warps = 8;
+    while (warps > 1 && dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget)
+        warps >>= 1;
+    pl.cta_slots = warps > 1 ? 2 * warps : 0;
+    uint32_t smem = dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(pl.cta_slots, pl.stride);
+    cudaError_t e;
+    switch (warps) {
+    case 8: e = plan_variant_fn<256>(c, pl, smem, k_dense<NW, 256>); break;
+    case 4: e = plan_variant_fn<128>(c, pl, smem, k_dense<NW, 128>); break;
+    case 2: e = plan_variant_fn<64>(c, pl, smem, k_dense<NW, 64>); break;
+    default: e = plan_variant_fn<32>(c, pl, smem, k_dense<NW, 32>); break;
+    }
+    if (e != cudaSuccess) return e;
+    pl.num_su = pl.grid * (pl.block / 32);
+    pl.global_ws = false;
+    pl.dense = true;
+    return cudaSuccess;
+}
+
+cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl)
+{
+    pl.dense = false;
+    // dense bitsets up to 255 vertices (degrees are bytes, 0xFF marks a removed vertex)
+    if (nmax <= 64 && !c.force_sparse) return plan_dense<2>(c, pl);
+    if (nmax <= 128 && !c.force_sparse) return plan_dense<4>(c, pl);
+    if (nmax <= 255 && !c.force_sparse) return plan_dense<8>(c, pl);
     pl.np = np;
     pl.su_bytes = su_workspace_bytes(np);
     pl.stride = (4 + np / 32 + 3) / 4 * 4;
@@ -226,7 +304,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     }
     uint32_t np = std::max<uint32_t>(32, (nmax + 31) / 32 * 32);
     Plan pl;
-    if (make_plan(c, np, pl) != cudaSuccess) return VC_ERR_CUDA;
+    if (make_plan(c, np, nmax, pl) != cudaSuccess) return VC_ERR_CUDA;
     const uint32_t stride = pl.stride;
     uint32_t q = 1024;
     while (q < 2 * pl.num_su) q <<= 1;
@@ -378,7 +456,8 @@ extern "C" uint32_t vc_debug_stats(int32_t device, int32_t enable, uint64_t *row
     Ctx *c = get_ctx(device, &err);
     if (!c) return 0;
     std::lock_guard<std::mutex> lk(c->mu);
-    if (enable >= 0) c->stats_on = enable != 0;
+    if (enable >= 0) c->stats_on = (enable & 1) != 0;
+    if (enable >= 0) c->force_sparse = (enable & 2) != 0;
     uint32_t nsu = c->last_num_su;
     if (rows) {
         uint32_t k = std::min(nsu, max_rows);
@@ -389,7 +468,7 @@ extern "C" uint32_t vc_debug_stats(int32_t device, int32_t enable, uint64_t *row
         launch_shape[1] = c->last_plan.block;
         launch_shape[2] = c->last_plan.smem;
         launch_shape[3] = c->last_plan.num_su;
-        launch_shape[4] = c->last_plan.np;
+        launch_shape[4] = c->last_plan.np | (c->last_plan.dense ? 0x80000000u : 0u);
     }
     return nsu;
 }

@@ -84,4 +84,14 @@ VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
     return (b + 15u) & ~15u;
 }
 
+// Dense-bitset search unit (graphs of at most 255 vertices, nw <= 8 words):
+// per CTA adj[32*nw][nw] u32; per warp
+//   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 | degs[32*nw] u8
+VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * nw; }
+VC_HD inline uint32_t dense_workspace_bytes(uint32_t nw)
+{
+    uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 32u * nw;
+    return (b + 15u) & ~15u;
+}
+
 }  // namespace vcg
