@@ -101,6 +101,8 @@ typedef struct vc_result {
     uint64_t tree_nodes;  /* search-tree nodes whose reduction fixpoint was computed */
     float kernel_ms;      /* device time of the search launch */
     float total_ms;       /* wall time of the call, copies included */
+    float done_ms;        /* from the launch's start until this graph finished */
+    uint32_t reserved;
 } vc_result;
 
 /* Plain one-graph solve; replaces the host path of main.cu:101-359 (device

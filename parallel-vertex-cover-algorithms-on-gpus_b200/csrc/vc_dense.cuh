@@ -495,6 +495,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
     s.c_best = 0;
     s.top = 0;
     s.deadline = globaltimer() + P.time_limit_ns;
+    if (lane_id() == 0) atomicCAS(&P.ctl[kT0], 0ull, globaltimer());
     s.stat = SUStat{0, 0, 0, 0, 0, 0, 0, 0, 0};
     unsigned long long nodes_total = 0;
     long long t_mark = clock64();

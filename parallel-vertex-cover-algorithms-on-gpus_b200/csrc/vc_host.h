@@ -48,7 +48,7 @@ struct Ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf rp, col, inst, st, covers, ctl, seq, data, gws, launches;
     PinBuf h_st, h_desc, h_covers;
-    unsigned long long h_ctl = 0;
+    unsigned long long h_ctl[vcg::kCtlWords] = {};
     bool stats_on = false;
     bool force_sparse = false;
     DevBuf stats;
@@ -67,6 +67,7 @@ struct Job {
     std::vector<vcg::InstState> st;
     std::vector<uint32_t> covers;
     float kernel_ms = 0;
+    unsigned long long t0 = 0;
     bool aborted = false;
     Plan plan;
 };

@@ -591,7 +591,11 @@ __device__ __forceinline__ void finish_stint(S &s, const Params &P)
         atomicAdd(&st.nodes, s.local_nodes);
         __threadfence();
         uint32_t old = atomicSub(&st.act, 1u);
-        if (old == 1u) atomicOr(&st.flags, kDone);
+        if (old == 1u) {
+            st.t_done = globaltimer();
+            __threadfence();
+            atomicOr(&st.flags, kDone);
+        }
     }
     s.local_nodes = 0;
     s.inst = kNone;
@@ -748,6 +752,7 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
     s.local_nodes = 0;
     s.c_best = 0;
     s.deadline = globaltimer() + P.time_limit_ns;
+    if (G::rank() == 0) atomicCAS(&P.ctl[kT0], 0ull, globaltimer());
     s.stat = SUStat{0, 0, 0, 0, 0, 0, 0, 0, 0};
     unsigned long long nodes_total = 0;
     long long t_mark = clock64();

@@ -100,6 +100,7 @@ __global__ void k_init_state(InstState *st, const InstDesc *d, uint32_t count)
         s.cover_size = kNone;
         s.pad = 0;
         s.nodes = 0;
+        s.t_done = 0;
         st[i] = s;
     }
 }
@@ -367,10 +368,10 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     cudaMemcpyAsync(c.h_covers.p, c.covers.p, sizeof(uint32_t) * std::max<uint32_t>(cover_words, 1),
                     cudaMemcpyDeviceToHost, stream);
     unsigned long long abort_flag = 0;
-    cudaMemcpyAsync(&c.h_ctl, (unsigned long long *)c.ctl.p + kAbort, sizeof(unsigned long long),
-                    cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(c.h_ctl, c.ctl.p, sizeof(unsigned long long) * kCtlWords, cudaMemcpyDeviceToHost, stream);
     if (cudaStreamSynchronize(stream) != cudaSuccess) return VC_ERR_CUDA;
-    abort_flag = c.h_ctl;
+    abort_flag = c.h_ctl[kAbort];
+    job.t0 = c.h_ctl[kT0];
     cudaEventElapsedTime(&job.kernel_ms, c.ev0, c.ev1);
     job.aborted = abort_flag != 0;
     job.st.assign((InstState *)c.h_st.p, (InstState *)c.h_st.p + count);
@@ -399,6 +400,7 @@ vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out)
     out->status = st;
     out->tree_nodes = s.nodes;
     out->kernel_ms = job.kernel_ms;
+    out->done_ms = (s.t_done && job.t0 && s.t_done >= job.t0) ? (float)((s.t_done - job.t0) * 1e-6) : 0.0f;
     bool have_cover = s.cover_size != kNone;
     if (d.mode == kModeMVC) {
         out->decision = 1;

@@ -23,7 +23,7 @@ constexpr uint32_t kError = 8u;   // a bounded wait gave up
 constexpr uint32_t kCut = 16u;    // work was dropped at the launch's time limit
 
 // control words, each on its own 128-byte line (index in u64 units)
-enum : uint32_t { kHead = 0, kTail = 16, kState = 32, kCursor = 48, kAbort = 64, kFinish = 80, kCtlWords = 96 };
+enum : uint32_t { kHead = 0, kTail = 16, kState = 32, kCursor = 48, kAbort = 64, kFinish = 80, kT0 = 96, kCtlWords = 112 };
 
 enum : uint32_t { kModeMVC = 0, kModePVC = 1 };
 
@@ -51,6 +51,7 @@ struct InstState {
     uint32_t cover_size;  // size of the cover in the bitmap, kNone = none
     uint32_t pad;
     unsigned long long nodes;
+    unsigned long long t_done;  // %globaltimer when the last token returned
 };
 
 struct Params {

@@ -49,7 +49,8 @@ class Request(ctypes.Structure):
 class Result(ctypes.Structure):
     _fields_ = [("size", ctypes.c_uint32), ("decision", ctypes.c_uint32), ("has_cover", ctypes.c_uint32),
                 ("status", ctypes.c_int), ("cover_mask", ctypes.c_void_p), ("tree_nodes", ctypes.c_uint64),
-                ("kernel_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+                ("kernel_ms", ctypes.c_float), ("total_ms", ctypes.c_float), ("done_ms", ctypes.c_float),
+                ("reserved", ctypes.c_uint32)]
 
 
 @dataclasses.dataclass
@@ -61,6 +62,7 @@ class Solution:
     tree_nodes: int
     kernel_ms: float
     total_ms: float
+    done_ms: float = 0.0
 
     @property
     def status_name(self) -> str:
@@ -129,7 +131,7 @@ def _request(instance: str, k: int, ub: int, node_limit: int, time_limit: float,
 def _solution(res: Result, cover: Optional[np.ndarray], n: int) -> Solution:
     return Solution(int(res.status), int(res.size), int(res.decision),
                     cover.astype(bool) if (cover is not None and res.has_cover) else None,
-                    int(res.tree_nodes), float(res.kernel_ms), float(res.total_ms))
+                    int(res.tree_nodes), float(res.kernel_ms), float(res.total_ms), float(res.done_ms))
 
 
 def solve(g, instance: str = "mvc", k: int = 0, ub: int = 0, node_limit: int = 0, time_limit: float = 0.0,
@@ -174,24 +176,24 @@ def _arena_struct(arena) -> CsrArena:
     return a
 
 
-def _batch_requests(count: int, instances, ks, ubs, node_limit, time_limit, flags, device):
+def _batch_requests(count: int, instances, ks, ubs, node_limit, time_limit, flags, device, stream=0):
     reqs = (Request * count)()
     for i in range(count):
         inst = instances[i] if isinstance(instances, (list, tuple)) else instances
         reqs[i] = _request(inst, ks[i] if ks is not None else 0, ubs[i] if ubs is not None else 0,
-                           node_limit, time_limit, flags, device)
+                           node_limit, time_limit, flags, device, stream)
     return reqs
 
 
 def solve_batch(arena, instances="mvc", ks: Optional[Sequence[int]] = None, ubs: Optional[Sequence[int]] = None,
                 node_limit: int = 0, time_limit: float = 0.0, want_cover: bool = True, device: int = -1,
-                d_row_ptr: int = 0, d_col: int = 0, validate: bool = True):
+                d_row_ptr: int = 0, d_col: int = 0, validate: bool = True, stream: int = 0):
     """Every graph of a workloads.Arena in one launch (vc_solve_batch, or
     vc_solve_batch_device when d_row_ptr/d_col point at a device copy).
     Returns (call status, [Solution])."""
     count = arena.count
     flags = 0 if validate else VC_FLAG_NO_VALIDATE
-    reqs = _batch_requests(count, instances, ks, ubs, node_limit, time_limit, flags, device)
+    reqs = _batch_requests(count, instances, ks, ubs, node_limit, time_limit, flags, device, stream)
     outs = (Result * count)()
     covers = []
     for i in range(count):
