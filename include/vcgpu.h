@@ -135,6 +135,22 @@ vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req,
 vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out);
 vc_status vc_server_destroy(vc_server *s);
 
+/* Solve one graph of at most 255 vertices without allocating any memory (no
+ * counterpart in the reference).  For callers that may not call cudaMalloc --
+ * code whose device memory is owned by a framework's pool, hosts that forbid
+ * allocation after start-up, callers that cannot afford an allocation's
+ * implicit synchronisation.  The graph (g->row_ptr, g->col) must be in device
+ * memory and req->flags must include VC_FLAG_DEVICE_INPUT.  Runs asynchronously
+ * on req->stream; writes 8 words to the caller's device buffer d_result
+ * (status, size, decision, has_cover, tree nodes low, tree nodes high, 0, 0)
+ * and, if d_cover is not NULL, the cover as ceil(n/32) bitmap words.  All
+ * scratch lives in one fixed 256 KiB device array per GPU (held until the
+ * process exits) that every call shares: calls that overlap on the GPU race and
+ * must be serialised by the caller.  The first call on a device does that
+ * device's set-up and should come before any stream capture.  Larger graphs
+ * return VC_ERR_TOO_LARGE. */
+vc_status vc_solve_noalloc(const vc_csr *g, const vc_request *req, uint32_t *d_result, uint32_t *d_cover);
+
 /* Diagnostics: the kernels launched by this library since load (for checking
  * that the device path ran), and a static status string. */
 uint64_t vc_kernel_launches(void);
