@@ -125,12 +125,18 @@ vc_status vc_solve_batch_device(const vc_csr_arena *arena, const uint32_t *d_row
 
 /* Continuous-batching server (no counterpart in the reference).  A persistent
  * kernel admits requests while others run; graphs and search state stay on the
- * device.  mem_budget_bytes bounds the device arena used by admitted requests
- * (0 = library default).  submit copies the graph and returns a ticket; poll
- * returns VC_PENDING until the ticket's result is ready, then fills *out
- * (out->cover_mask, if non-NULL, receives n bytes) and releases the ticket. */
+ * device.  mem_budget_bytes bounds the device arena holding admitted graphs
+ * (0 = 1 GiB); max_requests is the number of device slots (0 = 1024);
+ * max_vertices is the largest graph accepted (0 = 2048; <= 255 selects the
+ * dense-bitset kernel).  A request is admitted when a slot and arena room for
+ * its CSR are free.  submit validates and copies the graph and returns a
+ * ticket; poll returns VC_PENDING until the ticket's result is ready, then
+ * fills *out (out->cover_mask, if non-NULL, receives n bytes; total_ms is the
+ * time from submit to completion) and releases the ticket.  While a server
+ * runs on a device, its persistent kernel holds that device's SMs. */
 typedef struct vc_server vc_server;
-vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests, vc_server **out);
+vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests, uint32_t max_vertices,
+                           vc_server **out);
 vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket);
 vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out);
 vc_status vc_server_destroy(vc_server *s);

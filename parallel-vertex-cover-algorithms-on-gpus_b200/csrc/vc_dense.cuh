@@ -44,7 +44,8 @@ struct DSU {
     uint8_t *degs;        // [32*NW]
     uint32_t L[NW];
     const uint32_t *rp, *cl;
-    uint32_t inst, n, nw, mode, k;
+    uint32_t inst, n, nw, mode, k, cover_off;
+    unsigned long long node_limit;
     uint32_t base_del, top;
     uint32_t c_best;
     uint32_t fr_bot, fr_top;
@@ -250,12 +251,14 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
 template <class G, int NW>
 __device__ __forceinline__ void bind_graph(DSU<NW> &s, const Params &P, uint32_t inst)
 {
-    const InstDesc &d = P.inst[inst];
+    const InstDesc d = load_desc(&P.inst[inst]);
     s.inst = inst;
     s.n = d.n;
     s.nw = d.nw;
     s.mode = d.mode;
     s.k = d.k;
+    s.cover_off = d.cover_off;
+    s.node_limit = d.node_limit;
     s.rp = P.row_ptr + d.row_off;
     s.cl = P.col + d.col_off;
     s.fr_bot = s.fr_top = 0;
@@ -330,15 +333,15 @@ template <int NW>
 __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint32_t inst)
 {
     const unsigned lane = lane_id();
-    const InstDesc &d = P.inst[inst];
+    const InstDesc d = load_desc(&P.inst[inst]);
     const uint32_t *rp = P.row_ptr + d.row_off, *cl = P.col + d.col_off;
     for (uint32_t i = lane; i < 32u * NW * NW; i += 32) adj[i] = 0;
     __syncwarp();
     for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
         uint32_t *row = adj + v * NW;
-        const uint32_t e1 = __ldg(&rp[v + 1]);
-        for (uint32_t e = __ldg(&rp[v]); e < e1; ++e) {
-            const uint32_t u = __ldg(&cl[e]);
+        const uint32_t e1 = __ldcg(&rp[v + 1]);
+        for (uint32_t e = __ldcg(&rp[v]); e < e1; ++e) {
+            const uint32_t u = __ldcg(&cl[e]);
             row[u >> 5] |= 1u << (u & 31u);
         }
     }
@@ -389,16 +392,20 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
                     atomicExch(&cp.hdr[kCpExit], 1u);
                     res = 3;
                 } else if (cta_idle && !vld(&cp.hdr[kCpCursorClosed])) {
-                    uint32_t i = (uint32_t)atomicAdd(&P.ctl[kCursor], 1ull);
-                    if (i < P.count) {
+                    uint32_t i = kNone;
+                    if (claim_root(P, i)) {
+                        if (vld(&cp.hdr[kCpRegistered])) {
+                            atomicAdd(&P.ctl[kState], 0xffffffffffffffffull);  // idle CTAs-1
+                            cp.hdr[kCpRegistered] = 0u;
+                        }
                         atomicSub(&cp.hdr[kCpIdle], 1u);
                         slot = i;
                         res = 4;
-                    } else {
+                    } else if (!P.server) {
                         cp.hdr[kCpCursorClosed] = 1u;
                     }
                 }
-                if (res == 0 && vld(&cp.hdr[kCpCursorClosed])) {
+                if (res == 0 && (P.server || vld(&cp.hdr[kCpCursorClosed]))) {
                     unsigned long long stw = ld_relaxed_u64(&P.ctl[kState]);
                     if (!vld(&cp.hdr[kCpRegistered]) && cta_idle) {
                         stw = atomicAdd(&P.ctl[kState], 1ull) + 1ull;
@@ -411,7 +418,8 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
                         cp.hdr[kCpRegistered] = 0u;
                         atomicSub(&cp.hdr[kCpIdle], 1u);
                         res = 2;
-                    } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0) {
+                    } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0 &&
+                               (!P.server || server_may_stop(P))) {
                         atomicExch(&P.ctl[kFinish], 1ull);
                         atomicExch(&cp.hdr[kCpExit], 1u);
                         res = 3;
@@ -428,9 +436,10 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
         if (res == 3) return false;
         if (res == 4) {  // a new graph root for the whole CTA
             slot = G::bcast(slot);
-            if (vld(&cp.hdr[kCpStaged]) != slot) {
+            const uint32_t key = __ldcg(&P.inst[slot].key);
+            if (vld(&cp.hdr[kCpStaged]) != key) {
                 stage_graph<NW>(adj, P, slot);
-                if (lane == 0) cp.hdr[kCpStaged] = slot;
+                if (lane == 0) cp.hdr[kCpStaged] = key;
             }
             bind_graph<G>(s, P, slot);
             load_root<G>(s);
@@ -461,9 +470,10 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
             __syncwarp();
             __threadfence();
             const uint32_t inst = __ldcg(&g[0]);
-            if (vld(&cp.hdr[kCpStaged]) != inst) {
+            const uint32_t key = __ldcg(&P.inst[inst].key);
+            if (vld(&cp.hdr[kCpStaged]) != key) {
                 stage_graph<NW>(adj, P, inst);
-                if (lane == 0) cp.hdr[kCpStaged] = inst;
+                if (lane == 0) cp.hdr[kCpStaged] = key;
             }
             bind_graph<G>(s, P, inst);
             for (uint32_t w = lane; w < s.nw; w += 32) s.bits[w] = __ldcg(&g[4 + w]);
@@ -557,10 +567,9 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         s.local_nodes += 1;
         nodes_total += 1;
         if ((s.local_nodes & 1023ull) == 0ull) {
-            const InstDesc &d = P.inst[s.inst];
             if (lane == 0) {
                 unsigned long long tot = atomicAdd(&st.nodes, s.local_nodes) + s.local_nodes;
-                if (d.node_limit && tot >= d.node_limit) atomicOr(&st.flags, kBudget);
+                if (s.node_limit && tot >= s.node_limit) atomicOr(&st.flags, kBudget);
             }
             s.local_nodes = 0;
         }

@@ -225,6 +225,8 @@ extern "C" vc_status vc_solve_noalloc(const vc_csr *g, const vc_request *req, ui
     d.init_best = (d.mode == kModePVC) ? n + 1 : ((ub && ub < n) ? ub : n) + 1;
     d.cover_off = 0;
     d.node_limit = req->node_limit;
+    d.key = 0;
+    d.pad = 0;
 
     Scratch *s = su->scratch;
     k_noalloc_reset<<<(kRingSlots + 255) / 256, 256, 0, stream>>>(s, d);

@@ -68,6 +68,24 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p)
     return v;
 }
 
+// A graph descriptor read around L1 (server slots are rewritten during a launch).
+__device__ __forceinline__ InstDesc load_desc(const InstDesc *p)
+{
+    InstDesc d;
+    d.n = __ldcg(&p->n);
+    d.nw = __ldcg(&p->nw);
+    d.row_off = __ldcg(&p->row_off);
+    d.col_off = __ldcg(&p->col_off);
+    d.mode = __ldcg(&p->mode);
+    d.k = __ldcg(&p->k);
+    d.init_best = __ldcg(&p->init_best);
+    d.cover_off = __ldcg(&p->cover_off);
+    d.node_limit = __ldcg(&p->node_limit);
+    d.key = __ldcg(&p->key);
+    d.pad = 0;
+    return d;
+}
+
 // ---------------------------------------------------------------- groups
 struct WarpG {
     static constexpr unsigned kSize = 32;
@@ -155,7 +173,8 @@ struct SU {
     uint32_t *trail, *fpos, *fv, *marks, *bits, *ctr, *aux;
     // current graph
     const uint32_t *rp, *cl;
-    uint32_t inst, n, nw, mode, k;
+    uint32_t inst, n, nw, mode, k, cover_off;
+    unsigned long long node_limit;
     uint32_t base_del;
     uint32_t c_best;  // cached incumbent (refreshed every few nodes; stale values only weaken pruning)
     uint32_t fr_bot, fr_top;
@@ -385,12 +404,14 @@ __device__ __forceinline__ void rebuild(SU &s)
 template <class G>
 __device__ __forceinline__ void bind_graph(SU &s, const Params &P, uint32_t inst)
 {
-    const InstDesc &d = P.inst[inst];
+    const InstDesc d = load_desc(&P.inst[inst]);
     s.inst = inst;
     s.n = d.n;
     s.nw = d.nw;
     s.mode = d.mode;
     s.k = d.k;
+    s.cover_off = d.cover_off;
+    s.node_limit = d.node_limit;
     s.rp = P.row_ptr + d.row_off;
     s.cl = P.col + d.col_off;
     s.fr_bot = s.fr_top = 0;
@@ -542,12 +563,80 @@ __device__ bool donate_global(S &s, const Params &P)
     return true;
 }
 
+// Claims the next graph root (one thread).  Batch launches walk a cursor over
+// graphs 0..count-1; a server launch takes slot ids the host published on the
+// submission queue and initialises the slot's state.
+__device__ __forceinline__ bool claim_root(const Params &P, uint32_t &slot)
+{
+    if (!P.server) {
+        const uint32_t i = (uint32_t)atomicAdd(&P.ctl[kCursor], 1ull);
+        if (i < P.count) { slot = i; return true; }
+        return false;
+    }
+    for (int it = 0; it < 4; ++it) {
+        const unsigned long long c = ld_relaxed_u64(&P.ctl[kCursor]);
+        const unsigned long long t = ld_acquire_u64(&P.ctl[kSubTail]);
+        if (c >= t) return false;
+        if (atomicCAS(&P.ctl[kCursor], c, c + 1) == c) {
+            slot = __ldcg(&P.subq[c & P.subq_mask]);
+            const InstDesc d = load_desc(&P.inst[slot]);
+            InstState *st = &P.st[slot];
+            st->best = d.init_best;
+            st->act = 1;
+            st->flags = 0;
+            st->lock = 0;
+            st->cover_size = kNone;
+            st->nodes = 0;
+            st->t_done = 0;
+            __threadfence();
+            atomicExch(&P.ctl[kLastWork], globaltimer());
+            return true;
+        }
+    }
+    return false;
+}
+
+// True when a server launch may stop: the host asked for shutdown, or nothing
+// was submitted for idle_ns; and no published submission is unclaimed.
+__device__ __forceinline__ bool server_may_stop(const Params &P)
+{
+    if (ld_relaxed_u64(&P.ctl[kCursor]) < ld_acquire_u64(&P.ctl[kSubTail])) return false;
+    if (ld_relaxed_u64(&P.ctl[kShutdown])) return true;
+    return globaltimer() > ld_relaxed_u64(&P.ctl[kLastWork]) + P.idle_ns;
+}
+
+// Server mode: the SU that returned a graph's last token copies its result
+// and cover into the host-mapped record, then publishes the ticket.
+template <class G>
+__device__ __forceinline__ void publish_result(const Params &P, uint32_t slot)
+{
+    const InstDesc d = load_desc(&P.inst[slot]);
+    InstState *st = &P.st[slot];
+    HostResult *hr = reinterpret_cast<HostResult *>(P.hres + (size_t)slot * P.hres_words);
+    uint32_t *hcover = reinterpret_cast<uint32_t *>(hr + 1);
+    const uint32_t cs = ld_relaxed_u32(&st->cover_size);
+    if (cs != kNone)
+        for (uint32_t w = G::rank(); w < d.nw; w += G::kSize) hcover[w] = __ldcg(&P.covers[d.cover_off + w]);
+    __threadfence_system();
+    G::sync();
+    if (G::rank() == 0) {
+        hr->best = ld_relaxed_u32(&st->best);
+        hr->flags = ld_relaxed_u32(&st->flags);
+        hr->cover_size = cs;
+        hr->nodes = ld_relaxed_u64(&st->nodes);
+        hr->t_done = ld_relaxed_u64(&st->t_done);
+        __threadfence_system();
+        *reinterpret_cast<volatile unsigned long long *>(&hr->done) = d.key;
+        __threadfence_system();
+    }
+    G::sync();
+}
+
 // Record a cover found at a leaf (MVC improvement or PVC success).
 template <class G, class S>
 __device__ void report_leaf(S &s, const Params &P, uint32_t del)
 {
     InstState &st = P.st[s.inst];
-    const InstDesc &d = P.inst[s.inst];
     uint32_t write = 0;
     if (G::rank() == 0) {
         if (s.mode == kModeMVC) {
@@ -571,7 +660,7 @@ __device__ void report_leaf(S &s, const Params &P, uint32_t del)
     s.c_best = G::bcast(s.c_best);
     write = G::bcast(write);
     if (!write) return;
-    cover_bits<G>(s, P.covers + d.cover_off);
+    cover_bits<G>(s, P.covers + s.cover_off);
     __threadfence();
     G::sync();
     if (G::rank() == 0) {
@@ -586,6 +675,7 @@ __device__ void report_leaf(S &s, const Params &P, uint32_t del)
 template <class G, class S>
 __device__ __forceinline__ void finish_stint(S &s, const Params &P)
 {
+    uint32_t last = 0;
     if (G::rank() == 0) {
         InstState &st = P.st[s.inst];
         atomicAdd(&st.nodes, s.local_nodes);
@@ -595,7 +685,12 @@ __device__ __forceinline__ void finish_stint(S &s, const Params &P)
             st.t_done = globaltimer();
             __threadfence();
             atomicOr(&st.flags, kDone);
+            last = 1;
         }
+    }
+    if (P.server) {
+        last = G::bcast(last);
+        if (last) publish_result<G>(P, s.inst);
     }
     s.local_nodes = 0;
     s.inst = kNone;
@@ -627,16 +722,16 @@ template <class G, class S>
 __device__ bool acquire(S &s, const Params &P, CtaPool &cp, bool &cursor_open)
 {
     if (cursor_open) {
-        uint32_t i = 0;
-        if (G::rank() == 0) i = (uint32_t)atomicAdd(&P.ctl[kCursor], 1ull);
+        uint32_t i = kNone;
+        if (G::rank() == 0 && !claim_root(P, i)) i = kNone;
         i = G::bcast(i);
-        if (i < P.count) {
+        if (i != kNone) {
             bind_graph<G>(s, P, i);
             load_root<G>(s);
             s.stat.roots += 1;
             return true;
         }
-        cursor_open = false;
+        if (!P.server) cursor_open = false;
     }
     if (G::rank() == 0) {
         __threadfence_block();
@@ -677,7 +772,16 @@ __device__ bool acquire(S &s, const Params &P, CtaPool &cp, bool &cursor_open)
                         cp.hdr[kCpRegistered] = 1u;
                     }
                     const bool reg = vld(&cp.hdr[kCpRegistered]) != 0;
-                    if ((stw >> 32) > 0 && ring_claim_deq(P, qpos)) {
+                    uint32_t root = kNone;
+                    if (P.server && claim_root(P, root)) {  // a new submission
+                        if (reg) {
+                            atomicAdd(&P.ctl[kState], 0xffffffffffffffffull);  // idle CTAs-1
+                            cp.hdr[kCpRegistered] = 0u;
+                        }
+                        atomicSub(&cp.hdr[kCpIdle], 1u);
+                        slot = root;
+                        res = 4;
+                    } else if ((stw >> 32) > 0 && ring_claim_deq(P, qpos)) {
                         if (reg) {
                             atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle CTAs-1
                             cp.hdr[kCpRegistered] = 0u;
@@ -686,7 +790,8 @@ __device__ bool acquire(S &s, const Params &P, CtaPool &cp, bool &cursor_open)
                         }
                         atomicSub(&cp.hdr[kCpIdle], 1u);
                         res = 2;
-                    } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0) {
+                    } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0 &&
+                               (!P.server || server_may_stop(P))) {
                         atomicExch(&P.ctl[kFinish], 1ull);
                         atomicExch(&cp.hdr[kCpExit], 1u);
                         res = 3;
@@ -701,6 +806,13 @@ __device__ bool acquire(S &s, const Params &P, CtaPool &cp, bool &cursor_open)
         }
         res = G::bcast(res);
         if (res == 3) return false;
+        if (res == 4) {
+            slot = G::bcast(slot);
+            bind_graph<G>(s, P, slot);
+            load_root<G>(s);
+            s.stat.roots += 1;
+            return true;
+        }
         if (res == 1) {
             slot = G::bcast(slot);
             const uint32_t *d = cp.data + (size_t)slot * P.stride;
@@ -808,10 +920,9 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
         s.local_nodes += 1;
         nodes_total += 1;
         if ((s.local_nodes & 1023ull) == 0ull) {
-            const InstDesc &d = P.inst[s.inst];
             if (G::rank() == 0) {
                 unsigned long long tot = atomicAdd(&st.nodes, s.local_nodes) + s.local_nodes;
-                if (d.node_limit && tot >= d.node_limit) atomicOr(&st.flags, kBudget);
+                if (s.node_limit && tot >= s.node_limit) atomicOr(&st.flags, kBudget);
             }
             s.local_nodes = 0;
         }

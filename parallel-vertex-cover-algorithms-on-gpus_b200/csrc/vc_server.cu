@@ -1,0 +1,475 @@
+// vc_server.cu -- continuous-batching server (vc_server_* in include/vcgpu.h).
+//
+// One persistent search kernel per server runs on its own stream and keeps the
+// search state of every admitted request on the device.  A host thread (the
+// request loop):
+//   * admits submitted requests into device slots while a slot and arena memory
+//     are free (admission by the request's device bytes: its CSR plus its cover
+//     bitmap; the search state itself lives in the kernel's fixed per-SU
+//     workspaces), copies the graph and its descriptor on a copy stream, and
+//     publishes the slot id on the device submission queue;
+//   * relaunches the kernel when it has exited (it exits after an idle period)
+//     and work is waiting;
+//   * collects results, which the SU that returns a request's last work token
+//     writes into host-mapped memory, and frees the slot.
+// Requests that arrive while others run are claimed by idle search units at
+// once, so their work overlaps on the device with the requests in flight.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "vc_host.h"
+
+using namespace vcg;
+using namespace vch;
+
+namespace {
+
+struct Pending {
+    uint64_t ticket;
+    uint32_t n, m;
+    std::vector<uint32_t> rp, col;
+    vc_request req;
+    std::chrono::steady_clock::time_point t_submit;
+};
+
+struct SlotInfo {
+    uint64_t ticket = 0;
+    uint32_t n = 0, ub = 0, mode = 0, init_best = 0;
+    std::chrono::steady_clock::time_point t_submit;
+};
+
+struct Done {
+    vc_status status;
+    uint32_t size, decision, has_cover;
+    uint64_t nodes;
+    float total_ms;
+    std::vector<uint8_t> cover;
+};
+
+constexpr uint32_t kSubQ = 1u << 16;  // submission queue entries (power of two)
+
+}  // namespace
+
+struct vc_server {
+    int dev = -1;
+    Ctx *ctx = nullptr;
+    cudaStream_t kstream = nullptr, cstream = nullptr;
+    uint32_t slots = 0, nw_max = 0, max_n = 0;
+    uint64_t arena_cap = 0;
+    Plan pl;
+    uint32_t q = 0;
+    DevBuf desc, st, covers, ctl, seq, data, gws, subq, arena;
+    uint32_t *h_res = nullptr, *d_res = nullptr;
+    uint32_t res_words = 0;
+    // host state (guarded by mu)
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Pending> pending;
+    std::vector<uint32_t> free_slots;
+    std::vector<SlotInfo> info;
+    std::unordered_map<uint64_t, uint32_t> inflight;  // ticket -> slot
+    std::unordered_map<uint64_t, Done> done;
+    uint64_t next_ticket = 1;
+    uint64_t arena_bump = 0;
+    uint64_t sub_tail = 0;
+    bool running = false;
+    bool stop = false;
+    bool discard_queue = false;
+    vc_status fatal = VC_OK;
+    std::thread loop;
+};
+
+namespace {
+
+vc_status launch_kernel(vc_server *s)
+{
+    // fresh control words, keeping the submission queue's head and tail
+    unsigned long long ctl[kCtlWords];
+    memset(ctl, 0, sizeof(ctl));
+    unsigned long long head = 0;
+    if (cudaMemcpy(&head, (unsigned long long *)s->ctl.p + kCursor, sizeof(head), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return VC_ERR_CUDA;
+    // after a launch stopped at its time limit, unclaimed submissions were failed
+    // on the host: drop them from the queue
+    ctl[kCursor] = s->discard_queue ? s->sub_tail : head;
+    s->discard_queue = false;
+    ctl[kSubTail] = s->sub_tail;
+    if (cudaMemcpyAsync(s->ctl.p, ctl, sizeof(ctl), cudaMemcpyHostToDevice, s->cstream) != cudaSuccess) return VC_ERR_CUDA;
+    std::vector<unsigned long long> seq(s->q);
+    for (uint32_t i = 0; i < s->q; ++i) seq[i] = i;
+    if (cudaMemcpyAsync(s->seq.p, seq.data(), sizeof(unsigned long long) * s->q, cudaMemcpyHostToDevice, s->cstream) !=
+        cudaSuccess)
+        return VC_ERR_CUDA;
+    if (cudaStreamSynchronize(s->cstream) != cudaSuccess) return VC_ERR_CUDA;
+    Params P;
+    memset(&P, 0, sizeof(P));
+    P.row_ptr = (const uint32_t *)s->arena.p;
+    P.col = (const uint32_t *)s->arena.p;
+    P.inst = (const InstDesc *)s->desc.p;
+    P.st = (InstState *)s->st.p;
+    P.covers = (uint32_t *)s->covers.p;
+    P.count = 0;
+    P.num_su = s->pl.num_su;
+    P.ctl = (unsigned long long *)s->ctl.p;
+    P.pool_seq = (unsigned long long *)s->seq.p;
+    P.pool_data = (uint32_t *)s->data.p;
+    P.q_mask = s->q - 1;
+    P.stride = s->pl.stride;
+    P.np = s->pl.np;
+    P.su_bytes = s->pl.su_bytes;
+    P.cta_slots = s->pl.cta_slots;
+    P.gws = s->pl.global_ws ? (uint8_t *)s->gws.p : nullptr;
+    P.stats = nullptr;
+    P.time_limit_ns = 600ull * 1000000000ull;
+    P.server = 1;
+    P.subq_mask = kSubQ - 1;
+    P.subq = (const uint32_t *)s->subq.p;
+    P.hres = s->d_res;
+    P.hres_words = s->res_words;
+    P.idle_ns = 200ull * 1000000ull;
+    void *args[] = {&P};
+    if (cudaLaunchCooperativeKernel(s->pl.fn, dim3(s->pl.grid), dim3(s->pl.block), args, s->pl.smem, s->kstream) !=
+        cudaSuccess)
+        return VC_ERR_CUDA;
+    s->running = true;
+    return VC_OK;
+}
+
+// Admits pending requests into free slots (called by the loop, lock held):
+// copies their graphs and descriptors, then publishes their slot ids on the
+// submission queue with one synchronisation.  Returns the number admitted.
+uint32_t admit(vc_server *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
+{
+    arena_full = false;
+    std::vector<Pending> batch;
+    std::vector<uint32_t> published;
+    std::vector<InstDesc> descs;
+    while (!s->pending.empty() && !s->free_slots.empty() && batch.size() < 256) {
+        Pending &p = s->pending.front();
+        const uint64_t rows = p.n + 1, cols = std::max<uint64_t>(2ull * p.m, 1);
+        const uint64_t bytes = ((rows + cols) * 4 + 255) / 256 * 256;
+        if (bytes > s->arena_cap) {  // can never fit
+            s->done.emplace(p.ticket, Done{VC_ERR_NOMEM, 0, 0, 0, 0, 0.0f, {}});
+            s->pending.pop_front();
+            continue;
+        }
+        if (s->arena_bump + bytes > s->arena_cap) { arena_full = true; break; }
+        const uint32_t slot = s->free_slots.back();
+        s->free_slots.pop_back();
+        const uint64_t off = s->arena_bump / 4;
+        s->arena_bump += bytes;
+        InstDesc d;
+        memset(&d, 0, sizeof(d));
+        d.n = p.n;
+        d.nw = (p.n + 31) / 32;
+        d.row_off = off;
+        d.col_off = off + rows;
+        d.mode = p.req.instance == VC_PVC ? kModePVC : kModeMVC;
+        d.k = std::min<uint32_t>(p.req.k, p.n);
+        const uint32_t ub = p.req.instance == VC_MVC ? p.req.ub : 0;
+        d.init_best = d.mode == kModePVC ? p.n + 1 : ((ub && ub < p.n) ? ub : p.n) + 1;
+        d.cover_off = slot * s->nw_max;
+        d.node_limit = p.req.node_limit;
+        d.key = (uint32_t)p.ticket;
+        descs.push_back(d);
+        HostResult *hr = reinterpret_cast<HostResult *>(s->h_res + (size_t)slot * s->res_words);
+        hr->done = 0;  // the previous occupant's record
+        SlotInfo &si = s->info[slot];
+        si.ticket = p.ticket;
+        si.n = p.n;
+        si.ub = ub;
+        si.mode = d.mode;
+        si.init_best = d.init_best;
+        si.t_submit = p.t_submit;
+        s->inflight.emplace(p.ticket, slot);
+        published.push_back(slot);
+        batch.push_back(std::move(p));
+        s->pending.pop_front();
+    }
+    if (batch.empty()) return 0;
+    for (size_t i = 0; i < batch.size(); ++i) {
+        const Pending &p = batch[i];
+        const InstDesc &d = descs[i];
+        uint32_t *base = (uint32_t *)s->arena.p + d.row_off;
+        cudaMemcpyAsync(base, p.rp.data(), 4ull * (p.n + 1), cudaMemcpyHostToDevice, s->cstream);
+        if (p.m) cudaMemcpyAsync((uint32_t *)s->arena.p + d.col_off, p.col.data(), 8ull * p.m, cudaMemcpyHostToDevice, s->cstream);
+        cudaMemcpyAsync((InstDesc *)s->desc.p + published[i], &descs[i], sizeof(InstDesc), cudaMemcpyHostToDevice, s->cstream);
+    }
+    for (size_t i = 0; i < published.size(); ++i)
+        cudaMemcpyAsync((uint32_t *)s->subq.p + ((s->sub_tail + i) & (kSubQ - 1)), &published[i], 4,
+                        cudaMemcpyHostToDevice, s->cstream);
+    // graphs, descriptors and queue entries must land before the tail that publishes them
+    if (cudaStreamSynchronize(s->cstream) != cudaSuccess) { s->fatal = VC_ERR_CUDA; return 0; }
+    s->sub_tail += published.size();
+    unsigned long long tail = s->sub_tail;
+    cudaMemcpyAsync((unsigned long long *)s->ctl.p + kSubTail, &tail, sizeof(tail), cudaMemcpyHostToDevice, s->cstream);
+    if (cudaStreamSynchronize(s->cstream) != cudaSuccess) s->fatal = VC_ERR_CUDA;
+    (void)lk;
+    return (uint32_t)batch.size();
+}
+
+// Collects finished requests from the host-mapped records (lock held).
+uint32_t collect(vc_server *s)
+{
+    uint32_t got = 0;
+    std::vector<uint64_t> finished;
+    for (auto &kv : s->inflight) {
+        const uint32_t slot = kv.second;
+        const HostResult *hr = reinterpret_cast<const HostResult *>(s->h_res + (size_t)slot * s->res_words);
+        const unsigned long long done = *reinterpret_cast<const volatile unsigned long long *>(&hr->done);
+        if (done != (uint32_t)kv.first) continue;
+        std::atomic_thread_fence(std::memory_order_acquire);
+        const SlotInfo &si = s->info[slot];
+        Done d;
+        const uint32_t fl = hr->flags;
+        if (fl & kError) d.status = VC_ERR_INTERNAL;
+        else if (fl & kBudget) d.status = VC_BUDGET;
+        else if ((fl & kCut) || !(fl & kDone)) d.status = VC_TIMEOUT;
+        else d.status = VC_OK;
+        d.nodes = hr->nodes;
+        d.has_cover = hr->cover_size != kNone;
+        if (si.mode == kModeMVC) {
+            d.decision = 1;
+            d.size = hr->best < si.init_best ? hr->best : (si.ub ? si.ub : si.n);
+        } else {
+            d.decision = (fl & kFound) ? 1u : 0u;
+            d.size = d.decision ? hr->cover_size : 0u;
+        }
+        d.cover.assign(si.n, 0);
+        if (d.has_cover) {
+            const uint32_t *w = reinterpret_cast<const uint32_t *>(hr + 1);
+            for (uint32_t v = 0; v < si.n; ++v) d.cover[v] = (uint8_t)((w[v >> 5] >> (v & 31u)) & 1u);
+        }
+        d.total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - si.t_submit).count();
+        s->done.emplace(kv.first, std::move(d));
+        finished.push_back(kv.first);
+    }
+    for (uint64_t t : finished) {
+        const uint32_t slot = s->inflight[t];
+        s->inflight.erase(t);
+        s->free_slots.push_back(slot);
+        ++got;
+    }
+    return got;
+}
+
+// After an abnormal kernel exit, requests still in flight get a timeout status.
+void fail_inflight(vc_server *s, vc_status st)
+{
+    s->discard_queue = true;
+    for (auto &kv : s->inflight) {
+        Done d{st, 0, 0, 0, 0, 0.0f, {}};
+        s->done.emplace(kv.first, std::move(d));
+        s->free_slots.push_back(kv.second);
+    }
+    s->inflight.clear();
+}
+
+void request_loop(vc_server *s)
+{
+    cudaSetDevice(s->dev);
+    std::unique_lock<std::mutex> lk(s->mu);
+    uint32_t nap_us = 20;
+    while (true) {
+        if (s->fatal != VC_OK) {
+            fail_inflight(s, s->fatal);
+            for (auto &p : s->pending) s->done.emplace(p.ticket, Done{s->fatal, 0, 0, 0, 0, 0.0f, {}});
+            s->pending.clear();
+            s->cv.notify_all();
+            if (s->stop) break;
+            s->cv.wait_for(lk, std::chrono::milliseconds(5));
+            continue;
+        }
+        bool progress = false;
+        if (s->running && cudaStreamQuery(s->kstream) != cudaErrorNotReady) {
+            s->running = false;
+            // the kernel exited: everything it claimed has finished unless it stopped at its limit
+            collect(s);
+            unsigned long long abort_flag = 0;
+            cudaMemcpy(&abort_flag, (unsigned long long *)s->ctl.p + kAbort, sizeof(abort_flag), cudaMemcpyDeviceToHost);
+            if (abort_flag || cudaGetLastError() != cudaSuccess) fail_inflight(s, VC_TIMEOUT);
+            progress = true;
+        }
+        if (!s->stop) {
+            // The arena is a bump allocator whose addresses are never reused
+            // while one kernel launch runs (the search kernels read graphs
+            // through the non-coherent cache).  When it is full, in-flight work
+            // drains, the kernel is asked to stop, and the arena restarts empty.
+            if (!s->running && s->inflight.empty()) s->arena_bump = 0;
+            bool arena_full = false;
+            if (admit(s, lk, arena_full)) progress = true;
+            if (arena_full && s->inflight.empty() && s->running) {
+                unsigned long long one = 1;
+                cudaMemcpyAsync((unsigned long long *)s->ctl.p + kShutdown, &one, sizeof(one), cudaMemcpyHostToDevice,
+                                s->cstream);
+                cudaStreamSynchronize(s->cstream);
+            }
+            if (!s->inflight.empty() && !s->running) {
+                vc_status st = launch_kernel(s);
+                if (st != VC_OK) s->fatal = st;
+                progress = true;
+            }
+        }
+        if (collect(s)) progress = true;
+        if (progress) s->cv.notify_all();
+        if (s->stop && s->inflight.empty() && s->pending.empty()) break;
+        if (s->stop && !s->running) {
+            fail_inflight(s, VC_TIMEOUT);
+            break;
+        }
+        nap_us = progress ? 20 : std::min<uint32_t>(nap_us * 2, 500);
+        s->cv.wait_for(lk, std::chrono::microseconds(nap_us));
+    }
+    if (s->running) {  // ask the kernel to stop once idle and wait for it (bounded by its own limits)
+        unsigned long long one = 1;
+        cudaMemcpyAsync((unsigned long long *)s->ctl.p + kShutdown, &one, sizeof(one), cudaMemcpyHostToDevice,
+                        s->cstream);
+        cudaStreamSynchronize(s->cstream);
+        lk.unlock();
+        cudaStreamSynchronize(s->kstream);
+        lk.lock();
+        s->running = false;
+    }
+    s->cv.notify_all();
+}
+
+}  // namespace
+
+extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests,
+                                     uint32_t max_vertices, vc_server **out)
+{
+    if (!out) return VC_ERR_INVALID;
+    *out = nullptr;
+    vc_status err;
+    Ctx *c = get_ctx(device, &err);
+    if (!c) return err;
+    vc_server *s = new vc_server();
+    s->dev = c->dev;
+    s->ctx = c;
+    s->slots = max_requests ? max_requests : 1024;
+    const uint64_t budget = mem_budget_bytes ? mem_budget_bytes : (1ull << 30);
+    // the largest graph a request may have: it sizes the search units'
+    // workspaces and picks the kernel (dense bitsets up to 255 vertices)
+    const uint32_t max_n = max_vertices ? max_vertices : 2048;
+    if (max_n > kMaxVertices) { delete s; return VC_ERR_TOO_LARGE; }
+    s->max_n = max_n;
+    s->nw_max = (max_n + 31) / 32;
+    if (make_plan(*c, std::max<uint32_t>(32, (max_n + 31) / 32 * 32), max_n, s->pl) != cudaSuccess) {
+        delete s;
+        return VC_ERR_CUDA;
+    }
+    s->q = 1024;
+    while (s->q < 2 * s->pl.num_su) s->q <<= 1;
+    s->res_words = (uint32_t)(sizeof(HostResult) / 4) + s->nw_max;
+    s->res_words = (s->res_words + 3) / 4 * 4;
+    s->arena_cap = budget;
+    bool ok = cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && !s->desc.ensure(sizeof(InstDesc) * s->slots) && !s->st.ensure(sizeof(InstState) * s->slots) &&
+         !s->covers.ensure(4ull * s->slots * s->nw_max) && !s->ctl.ensure(sizeof(unsigned long long) * kCtlWords) &&
+         !s->seq.ensure(sizeof(unsigned long long) * s->q) && !s->data.ensure(4ull * s->q * s->pl.stride) &&
+         !s->subq.ensure(4ull * kSubQ) && !s->arena.ensure(budget) &&
+         (!s->pl.global_ws || !s->gws.ensure((size_t)s->pl.num_su * s->pl.su_bytes));
+    ok = ok && cudaMemset(s->ctl.p, 0, sizeof(unsigned long long) * kCtlWords) == cudaSuccess;
+    const size_t res_bytes = 4ull * s->slots * s->res_words;
+    ok = ok && cudaHostAlloc((void **)&s->h_res, res_bytes, cudaHostAllocMapped) == cudaSuccess;
+    ok = ok && cudaHostGetDevicePointer((void **)&s->d_res, s->h_res, 0) == cudaSuccess;
+    if (!ok) {
+        vc_server_destroy(s);
+        return VC_ERR_NOMEM;
+    }
+    memset(s->h_res, 0, res_bytes);
+    s->info.resize(s->slots);
+    for (uint32_t i = 0; i < s->slots; ++i) s->free_slots.push_back(s->slots - 1 - i);
+    s->loop = std::thread(request_loop, s);
+    *out = s;
+    return VC_OK;
+}
+
+extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket)
+{
+    if (!s || !g || !req || !ticket) return VC_ERR_INVALID;
+    if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
+    if (req->flags & VC_FLAG_DEVICE_INPUT) return VC_ERR_INVALID;  // the server copies from host memory
+    if (g->n == 0) return VC_ERR_INVALID;
+    if (g->n > s->max_n) return VC_ERR_TOO_LARGE;
+    if (!(req->flags & VC_FLAG_NO_VALIDATE)) {
+        vc_status v = validate_csr(g);
+        if (v != VC_OK) return v;
+    }
+    Pending p;
+    p.n = g->n;
+    p.m = g->m;
+    p.rp.assign(g->row_ptr, g->row_ptr + g->n + 1);
+    if (g->m) p.col.assign(g->col, g->col + 2ull * g->m);
+    p.req = *req;
+    p.t_submit = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return VC_ERR_INVALID;
+    if (s->fatal != VC_OK) return s->fatal;
+    p.ticket = s->next_ticket++;
+    *ticket = p.ticket;
+    s->pending.push_back(std::move(p));
+    s->cv.notify_all();
+    return VC_OK;
+}
+
+extern "C" vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out)
+{
+    if (!s || !out) return VC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->done.find(ticket);
+    if (it == s->done.end()) {
+        if (s->inflight.count(ticket)) return VC_PENDING;
+        for (auto &p : s->pending)
+            if (p.ticket == ticket) return VC_PENDING;
+        return VC_ERR_INVALID;
+    }
+    Done &d = it->second;
+    out->status = d.status;
+    out->size = d.size;
+    out->decision = d.decision;
+    out->has_cover = d.has_cover;
+    out->tree_nodes = d.nodes;
+    out->kernel_ms = 0;
+    out->total_ms = d.total_ms;
+    out->done_ms = d.total_ms;
+    if (out->cover_mask && !d.cover.empty()) memcpy(out->cover_mask, d.cover.data(), d.cover.size());
+    vc_status st = d.status;
+    s->done.erase(it);
+    return st;
+}
+
+extern "C" vc_status vc_server_destroy(vc_server *s)
+{
+    if (!s) return VC_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    if (s->loop.joinable()) s->loop.join();
+    s->desc.release();
+    s->st.release();
+    s->covers.release();
+    s->ctl.release();
+    s->seq.release();
+    s->data.release();
+    s->gws.release();
+    s->subq.release();
+    s->arena.release();
+    if (s->h_res) cudaFreeHost(s->h_res);
+    if (s->kstream) cudaStreamDestroy(s->kstream);
+    if (s->cstream) cudaStreamDestroy(s->cstream);
+    delete s;
+    return VC_OK;
+}

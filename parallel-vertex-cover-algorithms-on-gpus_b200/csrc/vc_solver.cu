@@ -332,6 +332,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     g_launches += 2;
 
     Params P;
+    memset(&P, 0, sizeof(P));
     P.row_ptr = job.d_rp;
     P.col = job.d_col;
     P.inst = (const InstDesc *)c.inst.p;
@@ -535,6 +536,8 @@ extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result 
     d.init_best = init_best_for(req, g->n);
     d.cover_off = 0;
     d.node_limit = req->node_limit;
+    d.key = 0;
+    d.pad = 0;
     job.desc.push_back(d);
     job.time_limit_s = req->time_limit_s;
     vc_status s = run_job(*c, job, stream);
@@ -614,6 +617,8 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         d.k = std::min<uint32_t>(reqs[i].k, d.n);
         d.init_best = init_best_for(&reqs[i], d.n);
         d.node_limit = reqs[i].node_limit;
+        d.key = i;
+        d.pad = 0;
         tl = std::max(tl, reqs[i].time_limit_s);
     }
     job.time_limit_s = tl;

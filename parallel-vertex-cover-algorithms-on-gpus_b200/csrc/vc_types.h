@@ -23,7 +23,13 @@ constexpr uint32_t kError = 8u;   // a bounded wait gave up
 constexpr uint32_t kCut = 16u;    // work was dropped at the launch's time limit
 
 // control words, each on its own 128-byte line (index in u64 units)
-enum : uint32_t { kHead = 0, kTail = 16, kState = 32, kCursor = 48, kAbort = 64, kFinish = 80, kT0 = 96, kCtlWords = 112 };
+enum : uint32_t {
+    kHead = 0, kTail = 16, kState = 32, kCursor = 48, kAbort = 64, kFinish = 80, kT0 = 96,
+    kSubTail = 112,   // server: submissions published by the host
+    kShutdown = 128,  // server: the host asks the kernel to exit once idle
+    kLastWork = 144,  // server: %globaltimer of the last claimed submission
+    kCtlWords = 160
+};
 
 enum : uint32_t { kModeMVC = 0, kModePVC = 1 };
 
@@ -41,6 +47,8 @@ struct InstDesc {
     uint32_t init_best;        // MVC: look for covers smaller than this
     uint32_t cover_off;        // word offset of this graph's cover bitmap
     uint64_t node_limit;       // 0 = none
+    uint32_t key;              // unique per graph (batch index / server ticket)
+    uint32_t pad;
 };
 
 struct InstState {
@@ -73,6 +81,21 @@ struct Params {
     uint8_t *gws;         // global workspace (CTA SUs on large graphs), else null
     unsigned long long *stats;    // per-SU counters (kStatWords each), null = off
     unsigned long long time_limit_ns;
+    // server mode (persistent kernel fed by the host)
+    uint32_t server;
+    uint32_t subq_mask;
+    const uint32_t *subq;         // slot ids in submission order
+    uint32_t *hres;               // host-mapped result records, hres_words u32 each
+    uint32_t hres_words;
+    unsigned long long idle_ns;   // exit after this long without any work
+};
+
+// Result record written by the device into host-mapped memory (server mode).
+struct HostResult {
+    unsigned long long done;      // ticket of the finished request (0 = none yet)
+    uint32_t best, flags, cover_size, pad;
+    unsigned long long nodes, t_done;
+    // followed by the cover bitmap words
 };
 
 // Workspace layout (bytes), np = vertex capacity, nw = np/32:

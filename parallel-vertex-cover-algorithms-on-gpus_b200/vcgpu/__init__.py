@@ -93,8 +93,12 @@ def lib():
         L.vc_debug_stats.restype = ctypes.c_uint32
         L.vc_status_string.argtypes = [ctypes.c_int]
         L.vc_status_string.restype = ctypes.c_char_p
+        if hasattr(L, "vc_solve_noalloc"):
+            L.vc_solve_noalloc.argtypes = [ctypes.POINTER(Csr), ctypes.POINTER(Request), ctypes.c_void_p,
+                                           ctypes.c_void_p]
+            L.vc_solve_noalloc.restype = ctypes.c_int
         if hasattr(L, "vc_server_create"):
-            L.vc_server_create.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint32,
+            L.vc_server_create.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
                                            ctypes.POINTER(ctypes.c_void_p)]
             L.vc_server_create.restype = ctypes.c_int
             L.vc_server_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(Csr), ctypes.POINTER(Request), _u64p]
@@ -228,3 +232,63 @@ def debug_stats(enable: Optional[bool] = None, device: int = -1):
 
 def kernel_launches() -> int:
     return int(lib().vc_kernel_launches())
+
+
+class Server:
+    """A continuous-batching server (vc_server_*): requests are admitted into a
+    persistent kernel while others run."""
+
+    def __init__(self, device: int = -1, mem_budget: int = 0, max_requests: int = 0, max_vertices: int = 0):
+        self._h = ctypes.c_void_p()
+        st = lib().vc_server_create(device, mem_budget, max_requests, max_vertices, ctypes.byref(self._h))
+        if st != VC_OK:
+            raise RuntimeError(f"vc_server_create failed: {STATUS_NAMES.get(st, st)}")
+        self._n = {}
+
+    def submit(self, g, instance: str = "mvc", k: int = 0, ub: int = 0, node_limit: int = 0,
+               validate: bool = True) -> int:
+        rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
+        col = np.ascontiguousarray(g.col, dtype=np.uint32)
+        c = Csr(g.n, col.shape[0] // 2, rp.ctypes.data, col.ctypes.data if col.size else None, None)
+        req = _request(instance, k, ub, node_limit, 0.0, 0 if validate else VC_FLAG_NO_VALIDATE, -1)
+        t = ctypes.c_uint64(0)
+        st = lib().vc_server_submit(self._h, ctypes.byref(c), ctypes.byref(req), ctypes.byref(t))
+        if st != VC_OK:
+            raise RuntimeError(f"vc_server_submit failed: {STATUS_NAMES.get(st, st)}")
+        self._n[t.value] = g.n
+        return int(t.value)
+
+    def poll(self, ticket: int, want_cover: bool = True) -> Optional[Solution]:
+        n = self._n[ticket]
+        res = Result()
+        cover = np.zeros(max(n, 1), dtype=np.uint8) if want_cover else None
+        res.cover_mask = cover.ctypes.data if cover is not None else None
+        st = lib().vc_server_poll(self._h, ticket, ctypes.byref(res))
+        if st == VC_PENDING:
+            return None
+        del self._n[ticket]
+        if st == VC_ERR_INVALID:
+            raise KeyError(ticket)
+        return _solution(res, cover[:n] if cover is not None else None, n)
+
+    def wait(self, ticket: int, timeout: float = 120.0, want_cover: bool = True) -> Solution:
+        import time
+        t0 = time.time()
+        while True:
+            r = self.poll(ticket, want_cover)
+            if r is not None:
+                return r
+            if time.time() - t0 > timeout:
+                raise TimeoutError(ticket)
+            time.sleep(0.0005)
+
+    def close(self):
+        if self._h:
+            lib().vc_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,114 @@
+"""The continuous-batching server: results are identical alone and in the mix,
+requests submitted while others run are admitted and overlap, and node
+budgets are honoured per request."""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+import oracle as O
+import vcgpu
+from vcgpu import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _mix(count, seed=0):
+    """Small-to-medium graphs of both families with their oracle optimum."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        i = int(rng.integers(0, 10**6))
+        if rng.random() < 0.5:
+            n = int(rng.integers(20, 90))
+            g = W.gnp(n, float(rng.uniform(3, 8)) / (n - 1), i)
+        else:
+            n = int(rng.integers(10, 40)) * 2
+            g = W.random_regular(n, 3, i)
+        st, opt, _, nodes = O.mvc(g, node_limit=200_000)
+        if st == O.OK:
+            out.append((g, opt))
+    return out
+
+
+def _check(g, r, instance, k, opt):
+    assert r.status == vcgpu.VC_OK, (g.name, r)
+    if instance == "mvc":
+        assert r.size == opt and r.cover is not None
+        assert W.is_cover(g, r.cover) and int(r.cover.sum()) == opt
+    else:
+        assert r.decision == (1 if opt <= k else 0), (g.name, k, opt)
+        if r.decision:
+            assert W.is_cover(g, r.cover) and int(r.cover.sum()) <= k
+
+
+@pytest.mark.parametrize("max_vertices", [255, 2048])
+def test_server_same_alone_and_in_mix(max_vertices):
+    items = _mix(40, seed=max_vertices)
+    jobs = []
+    for j, (g, opt) in enumerate(items):
+        if j % 3 == 0:
+            jobs.append((g, "pvc", opt - (j % 2), opt))
+        else:
+            jobs.append((g, "mvc", 0, opt))
+    with vcgpu.Server(max_vertices=max_vertices) as srv:
+        alone = []
+        for g, inst, k, opt in jobs[:8]:  # one at a time
+            t = srv.submit(g, inst, k=k)
+            alone.append(srv.wait(t))
+        tickets = [srv.submit(g, inst, k=k) for g, inst, k, opt in jobs]  # all at once
+        mixed = [srv.wait(t) for t in tickets]
+    for (g, inst, k, opt), r in zip(jobs, mixed):
+        _check(g, r, inst, k, opt)
+    for (g, inst, k, opt), a, m in zip(jobs[:8], alone, mixed[:8]):
+        _check(g, a, inst, k, opt)
+        assert (a.size, a.decision, a.status) == (m.size, m.decision, m.status)
+        # and the same as the plain one-graph entry point
+        p = vcgpu.solve(g, inst, k=k, time_limit=60.0)
+        assert (p.size, p.decision) == (m.size, m.decision)
+
+
+def test_server_admits_while_running():
+    """A long request runs while short ones arrive; the short ones finish first."""
+    recs = [json.loads(l) for l in open(os.path.join(GOLDEN, "batch_seed0.jsonl"))]
+    hard = sorted([r for r in recs if r["status"] == "ok" and 3_000_000 < r["nodes"] < 40_000_000],
+                  key=lambda r: r["i"])[0]
+    g_hard = W.batch_instance(hard["i"])
+    small = _mix(20, seed=5)
+    with vcgpu.Server(max_vertices=255) as srv:
+        th = srv.submit(g_hard, "mvc")
+        time.sleep(0.002)
+        ts = [srv.submit(g, "mvc") for g, _ in small]
+        rs = [srv.wait(t) for t in ts]
+        done_small = time.time()
+        rh = srv.wait(th)
+        done_hard = time.time()
+    for (g, opt), r in zip(small, rs):
+        _check(g, r, "mvc", 0, opt)
+    assert rh.status == vcgpu.VC_OK and rh.size == hard["opt"]
+    assert done_small <= done_hard
+    assert max(r.total_ms for r in rs) < rh.total_ms
+
+
+def test_server_node_budget_per_request():
+    recs = [json.loads(l) for l in open(os.path.join(GOLDEN, "batch_seed0.jsonl"))]
+    big = [r for r in recs if r["status"] == "ok" and r["nodes"] > 200_000][0]
+    g = W.batch_instance(big["i"])
+    small = _mix(5, seed=9)
+    with vcgpu.Server(max_vertices=255) as srv:
+        tb = srv.submit(g, "mvc", node_limit=5000)
+        ts = [srv.submit(h, "mvc") for h, _ in small]
+        rb = srv.wait(tb)
+        rs = [srv.wait(t) for t in ts]
+    assert rb.status == vcgpu.VC_BUDGET and rb.size >= big["opt"]
+    for (h, opt), r in zip(small, rs):
+        _check(h, r, "mvc", 0, opt)
+
+
+def test_server_rejects_oversize():
+    with vcgpu.Server(max_vertices=100) as srv:
+        with pytest.raises(RuntimeError):
+            srv.submit(W.gnp(150, 0.05, 1), "mvc")

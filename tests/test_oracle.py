@@ -1,0 +1,126 @@
+"""The CPU oracle, pinned: its restatement of the reference's sequential solver
+against (1) an independent brute force on every small graph, (2) the
+reference's own Sequential / SequentialParameterized compiled from its sources
+(oracle/_ref), (3) the reference's known answers (test/runGraphs.py:8-30) on the
+tractable graph files, and (4) the committed golden fixtures."""
+import itertools
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from vcgpu import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REF_ROOT = "/root/reference"
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference CPU solver not built")
+
+
+def brute_force_mvc(n, edges):
+    for size in range(n + 1):
+        for cover in itertools.combinations(range(n), size):
+            cs = set(cover)
+            if all(u in cs or v in cs for u, v in edges):
+                return size
+    return n
+
+
+def test_small_fixtures_match_brute_force():
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    rng = np.random.default_rng(0)
+    cases = small["exhaustive"]
+    pick = [cases[i] for i in sorted(set(rng.integers(0, len(cases), size=250).tolist()))]
+    for n, mask, opt in pick:
+        pairs = list(itertools.combinations(range(n), 2))
+        e = [pairs[j] for j in range(len(pairs)) if (mask >> j) & 1]
+        assert brute_force_mvc(n, e) == opt, (n, mask)
+        g = W.from_edges(n, np.asarray(e, dtype=np.int64).reshape(-1, 2))
+        st, size, cover, _ = O.mvc(g)
+        assert st == O.OK and size == opt and O.is_cover(g, cover) and int(cover.sum()) == opt
+
+
+def test_oracle_pvc_decisions_small():
+    for seed in range(30):
+        rng = np.random.default_rng(seed)
+        n = int(rng.integers(2, 9))
+        g = W.gnp(n, float(rng.uniform(0.1, 0.9)), seed)
+        opt = brute_force_mvc(n, [tuple(e) for e in g.edges().tolist()])
+        for k in range(0, n + 1):
+            st, found, cover, _ = O.pvc(g, k)
+            assert found == (opt <= k), (seed, k)
+            if found:
+                assert O.is_cover(g, cover) and int(cover.sum()) <= k
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(16))
+def test_restatement_equals_reference_gnp(seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(10, 70))
+    g = W.gnp(n, float(rng.uniform(0.03, 0.2)), 100 + seed)
+    st, opt, cover, _ = O.mvc(g)
+    assert st == O.OK
+    assert O.ref_mvc(g) == opt
+    assert O.ref_pvc(g, opt) == 1 and O.ref_pvc(g, max(opt - 1, 0)) == (1 if opt == 0 else 0)
+    assert O.pvc(g, opt)[1] == 1 and O.pvc(g, max(opt - 1, 0))[1] == (1 if opt == 0 else 0)
+
+
+@needs_ref
+def test_restatement_equals_reference_configs():
+    for g in (W.config1_graph(), W.config2_graph(), W.random_regular(60, 3, 5),
+              W.planted_cover(200, 40, 500, 20, 4, 3)):
+        st, opt, cover, _ = O.mvc(g)
+        assert st == O.OK and O.is_cover(g, cover)
+        assert O.ref_mvc(g) == opt, g.name
+        assert O.ref_remove_max_ub(g) >= opt
+
+
+@needs_ref
+def test_golden_batch_pinned_by_reference():
+    recs = [json.loads(l) for l in open(os.path.join(GOLDEN, "batch_seed0.jsonl"))]
+    easy = sorted([r for r in recs if r["status"] == "ok" and r["nodes"] <= 20000], key=lambda r: r["i"])[:40]
+    assert len(easy) >= 20
+    for r in easy:
+        g = W.batch_instance(r["i"])
+        assert (g.n, g.m) == (r["n"], r["m"])
+        assert O.ref_mvc(g) == r["opt"], r["i"]
+        st, opt, _, _ = O.mvc(g)
+        assert opt == r["opt"]
+
+
+def test_golden_small_configs():
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    g1, g2 = W.config1_graph(), W.config2_graph()
+    assert (g1.n, g1.m) == (small["config1"]["n"], small["config1"]["m"])
+    assert (g2.n, g2.m) == (small["config2"]["n"], small["config2"]["m"])
+    assert O.mvc(g1)[1] == small["config1"]["opt"]
+    assert O.mvc(g2)[1] == small["config2"]["opt"]
+    assert small["config2"]["pvc_k_opt"] == 1 and small["config2"]["pvc_k_opt_minus_1"] == 0
+
+
+KNOWN = ["cop_hat300-1.txt", "cop_hat300-2.txt"]
+
+
+@needs_ref
+@pytest.mark.skipif(not os.path.isdir(REF_ROOT), reason="reference tree absent")
+@pytest.mark.parametrize("fname", KNOWN)
+def test_known_answer_files(fname):
+    """test/runGraphs.py:8-30 lists the optimum of each graph file; the oracle
+    must reproduce it on the files it can solve in seconds."""
+    golden = json.load(open(os.path.join(GOLDEN, "known_answers.json")))["mvc"]
+    path = os.path.join(REF_ROOT, "test", "test_graphs", fname)
+    n, rp, col = O.ref_load(path)
+    g = W.Graph(n, rp, col, fname)
+    ours = W.read_reference_file(path)
+    assert np.array_equal(ours.row_ptr, rp) and np.array_equal(ours.col, col)
+    st, opt, cover, _ = O.mvc(g)
+    assert st == O.OK and opt == golden[fname] and O.is_cover(g, cover)
+
+
+def test_greedy_ub_is_a_cover():
+    for seed in range(10):
+        g = W.gnp(80, 0.08, seed)
+        ub, cover = O.greedy_ub(g)
+        assert O.is_cover(g, cover) and int(cover.sum()) == ub
