@@ -1,0 +1,69 @@
+"""The `output` command line (drop-in for the reference's ./output <args>)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from vcgpu import workloads as W
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(REPO, "parallel-vertex-cover-algorithms-on-gpus_b200", "output")
+needs_cli = pytest.mark.skipif(not os.path.exists(CLI), reason="output not built")
+
+
+def run(args, cwd):
+    return subprocess.run([CLI] + args, cwd=cwd, capture_output=True, text=True, timeout=120)
+
+
+@needs_cli
+def test_help_and_bad_options(tmp_path):
+    r = run(["-h"], tmp_path)
+    assert r.returncode == 0 and "-v <Version>" in r.stderr
+    r = run(["-x"], tmp_path)
+    assert r.returncode == 0 and "Unrecognized option" in r.stderr
+    r = run(["-v", "fast"], tmp_path)
+    assert r.returncode == 0 and "Unrecognized -v option" in r.stderr
+    r = run(["-i", "mis"], tmp_path)
+    assert r.returncode == 0 and "Unrecognized -i option" in r.stderr
+
+
+@needs_cli
+def test_sequential_refused(tmp_path):
+    r = run(["-v", "sequential", "-f", "x.txt"], tmp_path)
+    assert r.returncode == 1 and "not part of this build" in r.stderr
+
+
+@needs_cli
+@pytest.mark.parametrize("body,msg", [("3 1\n1 1\n", "self-loop"), ("3 2\n1 2\n2 1\n", "duplicate"),
+                                      ("3 1\n0 2\n", "out of range"), ("3 2\n1 2\n", "fewer edges"),
+                                      ("", "header")])
+def test_malformed_files(tmp_path, body, msg):
+    p = tmp_path / "g.txt"
+    p.write_text(body)
+    r = run(["-f", str(p)], tmp_path)
+    assert r.returncode == 1 and msg in r.stderr
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_solves_and_writes_results_row(tmp_path):
+    g = W.config1_graph()
+    p = tmp_path / "g60.txt"
+    W.write_reference_file(g, str(p))
+    opt = O.mvc(g)[1]
+    r = run(["-f", str(p), "-o", "run7"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert f"Size of minimum vertex cover: {opt}" in r.stdout
+    r = run(["-f", str(p), "-o", "run8", "-i", "pvc", "-k", str(opt - 1)], tmp_path)
+    assert r.returncode == 0 and f"Minimum is greater than K: {opt - 1}" in r.stdout
+    r = run(["-f", str(p), "-o", "run9", "-i", "pvc", "-k", str(opt)], tmp_path)
+    assert f"Minimum is less than or equal to K: {opt}" in r.stdout
+    rows = (tmp_path / "Results" / "Results.csv").read_text().strip().splitlines()
+    assert len(rows) == 3
+    f = rows[0].split(",")
+    assert len(f) == 22
+    assert f[0] == "run7" and f[2] == "60" and f[3] == str(g.m) and f[4] == "mvc" and f[5] == "hybrid"
+    assert f[6] == str(1 << 19) and f[18] == str(opt)
+    assert rows[1].split(",")[20] == "0" and rows[2].split(",")[20] == "1"
