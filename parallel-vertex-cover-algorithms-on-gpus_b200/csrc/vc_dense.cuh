@@ -29,18 +29,30 @@ namespace vcg {
 
 constexpr uint8_t kGone = 0xFFu;  // degs[] value of a removed vertex
 
+template <int NW>
+struct Rows {
+    static constexpr int kStride = NW >= 8 ? NW + 4 : NW;  // dense_row_words
+};
+
 // extra CTA header words used by the dense kernel
 enum : uint32_t { kCpStaged = 5, kCpCursorClosed = 6 };
+
+struct PhaseCycles {
+    unsigned long long scan, apply, pop, branch;
+};
 
 template <int NW>
 struct DSU {
     SUStat stat;
+    PhaseCycles cyc;
+    bool timed;
     const uint32_t *adj;  // CTA-shared [32*NW][NW]
     uint32_t *frames;     // [32*NW] (trail position << 16) | vertex
     uint32_t *marks;      // [NW]
     uint32_t *bits;       // [NW] record / scratch
     uint32_t *lsm;        // [NW] shared-memory mirror of L
     uint16_t *trail;      // [32*NW]
+    uint16_t *cand;       // [32*NW] degree-1/2 vertices of the current pass
     uint8_t *degs;        // [32*NW]
     uint32_t L[NW];
     const uint32_t *rp, *cl;
@@ -64,17 +76,23 @@ __device__ __forceinline__ void dsu_bind(DSU<NW> &s, uint8_t *ws, const uint32_t
     s.bits = s.marks + NW;
     s.lsm = s.bits + NW;
     s.trail = reinterpret_cast<uint16_t *>(s.lsm + NW);
-    s.degs = reinterpret_cast<uint8_t *>(s.trail + 32 * NW);
+    s.cand = s.trail + 32 * NW;
+    s.degs = reinterpret_cast<uint8_t *>(s.cand + 32 * NW);
 }
 
+// Loads the first nw (runtime, uniform) words of a row; the rest read as 0.
 template <int NW>
-__device__ __forceinline__ void load_row(const uint32_t *row, uint32_t (&r)[NW])
+__device__ __forceinline__ void load_row(const uint32_t *row, uint32_t (&r)[NW], uint32_t nw)
 {
     if constexpr (NW % 4 == 0) {
 #pragma unroll
         for (int w = 0; w < NW; w += 4) {
-            const uint4 q = *reinterpret_cast<const uint4 *>(row + w);
-            r[w] = q.x; r[w + 1] = q.y; r[w + 2] = q.z; r[w + 3] = q.w;
+            if ((uint32_t)w < nw) {
+                const uint4 q = *reinterpret_cast<const uint4 *>(row + w);
+                r[w] = q.x; r[w + 1] = q.y; r[w + 2] = q.z; r[w + 3] = q.w;
+            } else {
+                r[w] = r[w + 1] = r[w + 2] = r[w + 3] = 0u;
+            }
         }
     } else {
 #pragma unroll
@@ -100,13 +118,14 @@ template <int NW>
 __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
+    const int kmax = (int)s.nw;
 #pragma unroll 1
-    for (int k = 0; k < NW; ++k) {
+    for (int k = 0; k < kmax; ++k) {
         const uint32_t v = lane + 32u * k;
         uint8_t dv = kGone;
         if (v < s.n && ((s.lsm[k] >> lane) & 1u)) {
             uint32_t r[NW];
-            load_row<NW>(s.adj + v * NW, r);
+            load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
             uint32_t c = 0;
 #pragma unroll
             for (int w = 0; w < NW; ++w) c += __popc(r[w] & s.L[w]);
@@ -136,29 +155,6 @@ __device__ __forceinline__ void dense_push(DSU<NW> &s, const uint32_t (&M)[NW])
     mirror_L(s);
 }
 
-// Take the set M (subset of L): trail, L, and the degrees it changes.
-template <int NW>
-__device__ __forceinline__ void dense_remove(DSU<NW> &s, const uint32_t (&M)[NW])
-{
-    const unsigned lane = lane_id();
-    dense_push(s, M);
-#pragma unroll 1
-    for (int k = 0; k < NW; ++k) {
-        const uint32_t v = lane + 32u * k;
-        const uint8_t dv = s.degs[v];
-        if (dv == kGone) continue;
-        if (!((s.lsm[k] >> lane) & 1u)) { s.degs[v] = kGone; continue; }
-        if (dv == 0) continue;
-        uint32_t r[NW];
-        load_row<NW>(s.adj + v * NW, r);
-        uint32_t dec = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) dec += __popc(r[w] & M[w]);
-        if (dec) s.degs[v] = (uint8_t)(dv - dec);
-    }
-    __syncwarp();
-}
-
 // Put the trail above `pos` back into L.
 template <int NW>
 __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
@@ -178,73 +174,138 @@ __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
     __syncwarp();
 }
 
-// One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh).
+enum : int { kSweepKeep = 0, kSweepApply = 1, kSweepRecount = 2 };
+
+// One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh),
+// fused with the degree update it follows:
+//   kSweepRecount: degrees from scratch (after a pop, a received record, a root);
+//   kSweepApply:   the set M just left L (trail and L already updated):
+//                  subtract its edges from the live vertices, retire M;
+//   kSweepKeep:    degrees are current.
+// The same sweep takes the statistics and the high-degree marks and gathers the
+// degree-1/2 vertices with warp ballots; the gathered list is then worked one
+// vertex per lane.  Returns true if marks were made (left in s.marks).
 template <int NW>
-__device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
+__device__ __forceinline__ bool dense_pass(DSU<NW> &s, int mode, const uint32_t (&M)[NW], uint32_t del,
+                                           uint32_t bound, ScanOut &o)
 {
     const unsigned lane = lane_id();
     uint32_t sum = 0, maxd = 0, amax = kNone;
     bool marked = false;
+    uint32_t ncand = 0;
+    const int kmax = (int)s.nw;
 #pragma unroll 1
-    for (int k = 0; k < NW; ++k) {
+    for (int k = 0; k < kmax; ++k) {
         const uint32_t v = lane + 32u * k;
-        const uint32_t dv = s.degs[v];
-        if (dv == 0 || dv == kGone) continue;
-        sum += dv;
-        if (dv > maxd) { maxd = dv; amax = v; }
-        if (dv + del >= bound) {  // high-degree rule
-            atomicOr(&s.marks[k], 1u << lane);
-            marked = true;
-        } else if (dv <= 2) {     // degree-one / degree-two triangle rules
-            uint32_t r[NW];
-            load_row<NW>(s.adj + v * NW, r);
-            uint32_t n1 = kNone, n2 = kNone;
+        uint32_t dv = s.degs[v];
+        if (mode == kSweepRecount) {
+            if (v < s.n && ((s.lsm[k] >> lane) & 1u)) {
+                uint32_t r[NW];
+                load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+                uint32_t c = 0;
 #pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                uint32_t x = r[w] & s.L[w];
-                if (x && n2 == kNone) {
-                    const uint32_t u = 32u * w + (__ffs(x) - 1);
-                    if (n1 == kNone) {
-                        n1 = u;
-                        x &= x - 1;
-                        if (x) n2 = 32u * w + (__ffs(x) - 1);
-                    } else {
-                        n2 = u;
-                    }
+                for (int w = 0; w < NW; ++w) c += __popc(r[w] & s.L[w]);
+                dv = c;
+            } else {
+                dv = kGone;
+            }
+            s.degs[v] = (uint8_t)dv;
+        } else if (mode == kSweepApply && dv != kGone) {
+            if (!((s.lsm[k] >> lane) & 1u)) {
+                dv = kGone;
+                s.degs[v] = kGone;
+            } else if (dv != 0) {
+                uint32_t r[NW];
+                load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+                uint32_t dec = 0;
+#pragma unroll
+                for (int w = 0; w < NW; ++w) dec += __popc(r[w] & M[w]);
+                if (dec) {
+                    dv -= dec;
+                    s.degs[v] = (uint8_t)dv;
                 }
             }
-            if (dv == 1) {
-                const uint32_t du = s.degs[n1];
-                if (du > 1 || n1 < v) {
-                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
-                    marked = true;
+        }
+        bool cand = false;
+        if (dv != 0 && dv != kGone) {
+            sum += dv;
+            if (dv > maxd) { maxd = dv; amax = v; }
+            if (dv + del >= bound) {  // high-degree rule
+                atomicOr(&s.marks[k], 1u << lane);
+                marked = true;
+            } else {
+                cand = dv <= 2;
+            }
+        }
+        const uint32_t cm = __ballot_sync(0xffffffffu, cand);
+        if (cand) s.cand[ncand + __popc(cm & ((1u << lane) - 1u))] = (uint16_t)v;
+        ncand += __popc(cm);
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < ncand; i += 32) {  // degree-one / degree-two triangle rules
+        const uint32_t v = s.cand[i];
+        const uint32_t dv = s.degs[v];
+        uint32_t r[NW];
+        load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+        uint32_t n1 = kNone, n2 = kNone;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            uint32_t x = r[w] & s.L[w];
+            if (x && n2 == kNone) {
+                const uint32_t u = 32u * w + (__ffs(x) - 1);
+                if (n1 == kNone) {
+                    n1 = u;
+                    x &= x - 1;
+                    if (x) n2 = 32u * w + (__ffs(x) - 1);
+                } else {
+                    n2 = u;
                 }
-            } else if (n2 != kNone) {
-                const uint32_t d1 = s.degs[n1], d2 = s.degs[n2];
-                const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
-                if (!keep && ((s.adj[n2 * NW + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
-                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
-                    atomicOr(&s.marks[n2 >> 5], 1u << (n2 & 31u));
-                    marked = true;
-                }
+            }
+        }
+        if (dv == 1) {
+            const uint32_t du = s.degs[n1];
+            if (du > 1 || n1 < v) {
+                atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                marked = true;
+            }
+        } else if (n2 != kNone) {
+            const uint32_t d1 = s.degs[n1], d2 = s.degs[n2];
+            const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
+            if (!keep && ((s.adj[n2 * Rows<NW>::kStride + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
+                atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                atomicOr(&s.marks[n2 >> 5], 1u << (n2 & 31u));
+                marked = true;
             }
         }
     }
     s.stat.passes += 1;
     if (__any_sync(0xffffffffu, marked)) {
         __syncwarp();
-        uint32_t M[NW];
-#pragma unroll
-        for (int w = 0; w < NW; ++w) M[w] = s.marks[w];
-        __syncwarp();
-        if (lane < NW) s.marks[lane] = 0;
-        dense_remove(s, M);
         return true;
     }
     o.sum = __reduce_add_sync(0xffffffffu, sum);
     o.maxd = __reduce_max_sync(0xffffffffu, maxd);
     o.amax = __reduce_min_sync(0xffffffffu, (maxd == o.maxd && maxd > 0) ? amax : kNone);
     return false;
+}
+
+// Reduction to a fixpoint, starting with the given sweep mode and pending set.
+template <int NW>
+__device__ __forceinline__ void dense_reduce(DSU<NW> &s, int mode, uint32_t (&M)[NW], uint32_t bound, ScanOut &o)
+{
+    const unsigned lane = lane_id();
+#pragma unroll 1
+    for (int pass = 0; pass < 4 * 32 * NW; ++pass) {
+        if (!dense_pass(s, mode, M, s.base_del + s.top, bound, o)) break;
+        const long long t0 = s.timed ? clock64() : 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) M[w] = s.marks[w];
+        __syncwarp();
+        if (lane < NW) s.marks[lane] = 0;
+        dense_push(s, M);
+        mode = kSweepApply;
+        if (s.timed) s.cyc.apply += (unsigned long long)(clock64() - t0);
+    }
 }
 
 // ---- the overloads the shared work-sharing code (vc_search.cuh) calls
@@ -312,7 +373,7 @@ __device__ __forceinline__ void donation_bits(DSU<NW> &s)
         atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
     }
     __syncwarp();
-    if (lane < NW) s.bits[lane] &= ~s.adj[v * NW + lane];
+    if (lane < NW) s.bits[lane] &= ~s.adj[v * Rows<NW>::kStride + lane];
     __syncwarp();
 }
 
@@ -335,10 +396,10 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
     const unsigned lane = lane_id();
     const InstDesc d = load_desc(&P.inst[inst]);
     const uint32_t *rp = P.row_ptr + d.row_off, *cl = P.col + d.col_off;
-    for (uint32_t i = lane; i < 32u * NW * NW; i += 32) adj[i] = 0;
+    for (uint32_t i = lane; i < 32u * NW * Rows<NW>::kStride; i += 32) adj[i] = 0;
     __syncwarp();
     for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
-        uint32_t *row = adj + v * NW;
+        uint32_t *row = adj + v * Rows<NW>::kStride;
         const uint32_t e1 = __ldcg(&rp[v + 1]);
         for (uint32_t e = __ldcg(&rp[v]); e < e1; ++e) {
             const uint32_t u = __ldcg(&cl[e]);
@@ -507,27 +568,35 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
     s.deadline = globaltimer() + P.time_limit_ns;
     if (lane_id() == 0) atomicCAS(&P.ctl[kT0], 0ull, globaltimer());
     s.stat = SUStat{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    s.cyc = PhaseCycles{0, 0, 0, 0};
+    s.timed = P.stats != nullptr;
     unsigned long long nodes_total = 0;
     long long t_mark = clock64();
     bool have = false;
     uint32_t ticks = 0, c_flags = 0;
     unsigned long long c_state = 0;
     const unsigned lane = lane_id();
+    int sweep = kSweepKeep;  // how the next node's first pass brings degrees up to date
+    uint32_t pend[NW];       // the set that node's first pass subtracts (kSweepApply)
+#pragma unroll
+    for (int w = 0; w < NW; ++w) pend[w] = 0;
 
     for (;;) {
         if (!have) {
             if (s.inst != kNone && s.fr_top > s.fr_bot) {
+                const long long t_pop = s.timed ? clock64() : 0;
                 s.fr_top -= 1;
                 const uint32_t f = s.frames[s.fr_top];
                 const uint32_t v = f & 0xffffu;
                 dense_restore(s, f >> 16);
                 uint32_t N[NW];
-                load_row<NW>(s.adj + v * NW, N);
+                load_row<NW>(s.adj + v * Rows<NW>::kStride, N, NW);
 #pragma unroll
                 for (int w = 0; w < NW; ++w) N[w] &= s.L[w];
                 dense_push(s, N);
-                dense_degrees(s);
+                sweep = kSweepRecount;  // the child's first pass recounts
                 have = true;
+                if (s.timed) s.cyc.pop += (unsigned long long)(clock64() - t_pop);
             } else {
                 if (s.inst != kNone) finish_stint<G, S>(s, P);
                 long long t0 = clock64();
@@ -537,6 +606,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
                 s.stat.idle += (unsigned long long)(t_mark - t0);
                 if (!got) break;
                 have = true;
+                sweep = kSweepKeep;  // load_root / rebuild counted the degrees
                 ticks = 0;
             }
         }
@@ -566,7 +636,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         }
         s.local_nodes += 1;
         nodes_total += 1;
-        if ((s.local_nodes & 1023ull) == 0ull) {
+        if ((s.local_nodes & 127ull) == 0ull) {
             if (lane == 0) {
                 unsigned long long tot = atomicAdd(&st.nodes, s.local_nodes) + s.local_nodes;
                 if (s.node_limit && tot >= s.node_limit) atomicOr(&st.flags, kBudget);
@@ -576,9 +646,10 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         const uint32_t best = s.c_best;
         const uint32_t bound = s.mode == kModeMVC ? best : s.k + 1;
         ScanOut o = {0u, 0u, kNone};
-#pragma unroll 1
-        for (int pass = 0; pass < 4 * 32 * NW; ++pass)
-            if (!dense_pass(s, s.base_del + s.top, bound, o)) break;
+        const long long t_scan = s.timed ? clock64() : 0;
+        const unsigned long long apply0 = s.cyc.apply;
+        dense_reduce(s, sweep, pend, bound, o);
+        if (s.timed) s.cyc.scan += (unsigned long long)(clock64() - t_scan) - (s.cyc.apply - apply0);
         const uint32_t del = s.base_del + s.top;
         const uint64_t edges = o.sum / 2;
         bool prune;
@@ -601,6 +672,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
             have = false;
             continue;
         }
+        const long long t_br = s.timed ? clock64() : 0;
         const uint32_t v = o.amax;
         if (lane == 0) s.frames[s.fr_top] = (s.top << 16) | v;
         s.fr_top += 1;
@@ -614,10 +686,11 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         want = G::bcast(want);
         if (want == 1) donate_local<G, S>(s, P, cp);
         else if (want == 2 && donate_global<G, S>(s, P)) c_state += 1ull << 32;
-        uint32_t M[NW];
 #pragma unroll
-        for (int w = 0; w < NW; ++w) M[w] = ((uint32_t)w == (v >> 5)) ? (1u << (v & 31u)) : 0u;
-        dense_remove(s, M);
+        for (int w = 0; w < NW; ++w) pend[w] = ((uint32_t)w == (v >> 5)) ? (1u << (v & 31u)) : 0u;
+        dense_push(s, pend);
+        sweep = kSweepApply;  // the child's first pass subtracts v's edges
+        if (s.timed) s.cyc.branch += (unsigned long long)(clock64() - t_br);
     }
     if (P.stats && lane == 0) {
         unsigned long long *o = P.stats + (size_t)G::su_global() * kStatWords;
@@ -634,6 +707,11 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         o[kStPolls] = s.stat.polls;
         o[kStRestored] = s.stat.restored;
         o[kStSmid] = smid;
+        o[kStCycScan] = s.cyc.scan;
+        o[kStCycApply] = s.cyc.apply;
+        o[kStCycPop] = s.cyc.pop;
+        o[kStCycBranch] = s.cyc.branch;
+        o[kStCycOther] = s.stat.busy - s.cyc.scan - s.cyc.apply - s.cyc.pop - s.cyc.branch;
     }
 }
 

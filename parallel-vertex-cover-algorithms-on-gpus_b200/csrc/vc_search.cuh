@@ -671,6 +671,8 @@ __device__ void report_leaf(S &s, const Params &P, uint32_t del)
     }
 }
 
+__device__ __forceinline__ bool old_act_pending(InstState &st) { return ld_relaxed_u32(&st.act) > 1u; }
+
 // The SU leaves its current graph: return its token and node count.
 template <class G, class S>
 __device__ __forceinline__ void finish_stint(S &s, const Params &P)
@@ -680,6 +682,10 @@ __device__ __forceinline__ void finish_stint(S &s, const Params &P)
         InstState &st = P.st[s.inst];
         atomicAdd(&st.nodes, s.local_nodes);
         __threadfence();
+        if (s.node_limit) {
+            const unsigned long long tot = ld_relaxed_u64(&st.nodes);
+            if (tot >= s.node_limit && old_act_pending(st)) atomicOr(&st.flags, kBudget);
+        }
         uint32_t old = atomicSub(&st.act, 1u);
         if (old == 1u) {
             st.t_done = globaltimer();
@@ -919,7 +925,7 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
         }
         s.local_nodes += 1;
         nodes_total += 1;
-        if ((s.local_nodes & 1023ull) == 0ull) {
+        if ((s.local_nodes & 127ull) == 0ull) {
             if (G::rank() == 0) {
                 unsigned long long tot = atomicAdd(&st.nodes, s.local_nodes) + s.local_nodes;
                 if (s.node_limit && tot >= s.node_limit) atomicOr(&st.flags, kBudget);

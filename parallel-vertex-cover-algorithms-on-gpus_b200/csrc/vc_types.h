@@ -37,7 +37,9 @@ enum : uint32_t { kModeMVC = 0, kModePVC = 1 };
 // NODES_PER_SM histogram), written once when an SU exits, only when enabled.
 enum : uint32_t {
     kStNodes = 0, kStPasses, kStDonations, kStDonateFail, kStReceives, kStRoots, kStBusyCycles, kStIdleCycles,
-    kStPolls, kStRestored, kStSmid, kStatWords = 16
+    kStPolls, kStRestored, kStSmid,
+    kStCycScan, kStCycApply, kStCycPop, kStCycBranch, kStCycOther,  // dense search phases (clock64)
+    kStatWords = 16
 };
 
 struct InstDesc {
@@ -109,12 +111,16 @@ VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
 }
 
 // Dense-bitset search unit (graphs of at most 255 vertices, nw <= 8 words):
-// per CTA adj[32*nw][nw] u32; per warp
-//   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 | degs[32*nw] u8
-VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * nw; }
+// per CTA adj[32*nw][dense_row_words(nw)] u32; per warp
+//   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 |
+//   cand[32*nw] u16 | degs[32*nw] u8
+// Row stride in words: 8-word rows are padded to 12 so that the 16-byte row
+// loads of eight consecutive lanes fall in distinct shared-memory banks.
+VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw >= 8 ? nw + 4 : nw; }
+VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw); }
 VC_HD inline uint32_t dense_workspace_bytes(uint32_t nw)
 {
-    uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 32u * nw;
+    uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 2u * 32u * nw + 32u * nw;
     return (b + 15u) & ~15u;
 }
 
