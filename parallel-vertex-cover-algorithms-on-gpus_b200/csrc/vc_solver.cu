@@ -605,44 +605,64 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         job.d_rp = (const uint32_t *)c->rp.p;
         job.d_col = (const uint32_t *)c->col.p;
     }
-    job.desc.resize(count);
-    double tl = 0;
-    for (uint32_t i = 0; i < count; ++i) {
-        InstDesc &d = job.desc[i];
-        d.n = a->n[i];
-        d.nw = (d.n + 31) / 32;
-        d.row_off = a->row_off[i];
-        d.col_off = a->col_off[i];
-        d.mode = reqs[i].instance == VC_PVC ? kModePVC : kModeMVC;
-        d.k = std::min<uint32_t>(reqs[i].k, d.n);
-        d.init_best = init_best_for(&reqs[i], d.n);
-        d.node_limit = reqs[i].node_limit;
-        d.key = i;
-        d.pad = 0;
-        tl = std::max(tl, reqs[i].time_limit_s);
-    }
-    job.time_limit_s = tl;
-    vc_status s = run_job(*c, job, stream);
-    if (s != VC_OK) {
-        for (uint32_t i = 0; i < count; ++i) out[i].status = s;
-        return s;
-    }
+    // One launch per kernel shape: dense bitsets (n <= 255), warp search units
+    // (n <= kWarpMaxNP), CTA search units (larger); the shape is sized by the
+    // largest graph of its class, so small graphs never run in a large graph's
+    // workspace.
+    auto klass = [](uint32_t n) { return n <= 255 ? 0 : (n <= kWarpMaxNP ? 1 : 2); };
     vc_status first = VC_OK;
+    float total_kernel = 0;
+    std::vector<uint32_t> members;
+    for (int cl = 0; cl < 3; ++cl) {
+        members.clear();
+        for (uint32_t i = 0; i < count; ++i)
+            if (a->n[i] > 0 && klass(a->n[i]) == cl) members.push_back(i);
+        if (members.empty()) continue;
+        Job cj;
+        cj.d_rp = job.d_rp;
+        cj.d_col = job.d_col;
+        cj.desc.resize(members.size());
+        double tl = 0;
+        for (size_t j = 0; j < members.size(); ++j) {
+            const uint32_t i = members[j];
+            InstDesc &d = cj.desc[j];
+            d.n = a->n[i];
+            d.nw = (d.n + 31) / 32;
+            d.row_off = a->row_off[i];
+            d.col_off = a->col_off[i];
+            d.mode = reqs[i].instance == VC_PVC ? kModePVC : kModeMVC;
+            d.k = std::min<uint32_t>(reqs[i].k, d.n);
+            d.init_best = init_best_for(&reqs[i], d.n);
+            d.node_limit = reqs[i].node_limit;
+            d.key = (uint32_t)j;
+            d.pad = 0;
+            tl = std::max(tl, reqs[i].time_limit_s);
+        }
+        cj.time_limit_s = tl;
+        vc_status s = run_job(*c, cj, stream);
+        if (s != VC_OK) {
+            for (uint32_t i = 0; i < count; ++i) out[i].status = s;
+            return s;
+        }
+        total_kernel += cj.kernel_ms;
+        for (size_t j = 0; j < members.size(); ++j) {
+            const uint32_t i = members[j];
+            vc_status si = fill_result(cj, (uint32_t)j, reqs[i].instance == VC_MVC ? reqs[i].ub : 0, &out[i]);
+            if (si != VC_OK && first == VC_OK) first = si;
+        }
+    }
     float total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     for (uint32_t i = 0; i < count; ++i) {
+        out[i].total_ms = total;
+        out[i].kernel_ms = total_kernel;
         if (a->n[i] == 0) {
             out[i].status = VC_OK;
             out[i].size = 0;
             out[i].decision = 1;
             out[i].has_cover = 1;
             out[i].tree_nodes = 0;
-            out[i].kernel_ms = job.kernel_ms;
-            out[i].total_ms = total;
-            continue;
+            out[i].done_ms = 0;
         }
-        vc_status si = fill_result(job, i, reqs[i].instance == VC_MVC ? reqs[i].ub : 0, &out[i]);
-        out[i].total_ms = total;
-        if (si != VC_OK && first == VC_OK) first = si;
     }
     return first;
 }

@@ -80,6 +80,16 @@ def small():
     st, opt2, _, nodes2 = O.mvc(g2)
     out["config2"] = {"n": g2.n, "m": g2.m, "opt": opt2, "nodes": nodes2,
                       "pvc_k_opt": O.pvc(g2, opt2)[1], "pvc_k_opt_minus_1": O.pvc(g2, opt2 - 1)[1]}
+    g5 = W.chung_lu()
+    ub5, _ = O.greedy_ub(g5)
+    st, opt5, _, nodes5 = O.mvc(g5, ub=ub5 + 1)
+    out["config5"] = {"n": g5.n, "m": g5.m, "opt": opt5, "nodes": nodes5}
+    side = []
+    for i in range(512):
+        gs = W.gnp(100, 0.08, 10_000 + i)
+        st, o, _, nd = O.mvc(gs, node_limit=5_000_000)
+        side.append([10_000 + i, o if st == O.OK else None, nd])
+    out["config5_side"] = side
     # every graph on up to 6 vertices is enumerable; keep a seeded sample of 7-vertex ones
     rng = np.random.default_rng(0)
     small_cases = []
@@ -94,7 +104,8 @@ def small():
     out["exhaustive"] = small_cases
     with open(os.path.join(HERE, "small.json"), "w") as f:
         json.dump(out, f)
-    print("config1", out["config1"], "config2", out["config2"], "exhaustive", len(small_cases))
+    print("config1", out["config1"], "config2", out["config2"], "config5", out["config5"],
+          "side solved", sum(1 for x in side if x[1] is not None), "exhaustive", len(small_cases))
 
 
 def files():

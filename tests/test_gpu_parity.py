@@ -164,3 +164,55 @@ def test_empty_and_edgeless():
     assert r.status == vcgpu.VC_OK and r.size == 0 and not r.cover.any()
     r = vcgpu.solve(W.from_edges(7, np.zeros((0, 2))), "pvc", k=0, time_limit=TL)
     assert r.decision == 1
+
+
+def test_config5_chung_lu_plain_and_batched():
+    """Chung-Lu n=100000 (gamma 2.1, average degree 8, max degree 2000, seed 7),
+    plain, and batched alongside 512 G(100, 0.08) graphs."""
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    g = W.chung_lu()
+    assert (g.n, g.m) == (small["config5"]["n"], small["config5"]["m"])
+    opt = small["config5"]["opt"]
+    _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+    side = [(W.gnp(100, 0.08, s), o) for s, o, _ in small["config5_side"]]
+    graphs = [g] + [h for h, _ in side]
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    assert st == vcgpu.VC_OK
+    _check_mvc(g, sols[0], opt)
+    for (h, o), r in zip(side, sols[1:]):
+        _check_mvc(h, r, o)
+
+
+def test_mixed_size_classes_in_one_batch():
+    """Graphs for all three kernel shapes (dense <= 255 vertices, warp CSR units
+    up to 2048, CTA units above) in one batched call."""
+    rng = np.random.default_rng(77)
+    graphs, opts = [], []
+    for n in (40, 180, 300, 700, 1500, 2500, 3000):
+        g = W.gnp(n, 2.2 / (n - 1), int(rng.integers(1 << 30)))
+        st, opt, _, _ = O.mvc(g, node_limit=2_000_000)
+        assert st == O.OK
+        graphs.append(g)
+        opts.append(opt)
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    assert st == vcgpu.VC_OK
+    for g, r, opt in zip(graphs, sols, opts):
+        _check_mvc(g, r, opt)
+    for g, opt in zip(graphs, opts):  # and the plain entry point on each
+        _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+
+
+def test_csr_kernel_on_small_graphs():
+    """The CSR search (forced for graphs the dense kernel would take) stays exact."""
+    recs = _golden_batch(200_000)[:24]
+    graphs = [W.batch_instance(r["i"]) for r in recs]
+    vcgpu.debug_stats(2)  # force the CSR kernel
+    try:
+        st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+        single = vcgpu.solve(graphs[0], "pvc", k=recs[0]["opt"] - 1, time_limit=TL)
+    finally:
+        vcgpu.debug_stats(0)
+    assert st == vcgpu.VC_OK
+    for g, r, rec in zip(graphs, sols, recs):
+        _check_mvc(g, r, rec["opt"])
+    assert single.status == vcgpu.VC_OK and single.decision == 0
