@@ -209,7 +209,7 @@ def our_arm(args, world, rank, local, pg):
     import vcgpu
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    graphs = W.batch_graphs(args.count, seed=rank)
+    graphs = W.rank_batch(args.count, rank)
     arena = W.pack(graphs)
     n_arr = np.asarray([g.n for g in graphs], np.int64)
     m_arr = np.asarray([g.m for g in graphs], np.int64)

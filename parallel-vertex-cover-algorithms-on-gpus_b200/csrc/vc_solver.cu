@@ -565,10 +565,21 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
                               const uint32_t *d_col, std::chrono::steady_clock::time_point t0)
 {
     const uint32_t count = a->count;
+    // every early failure is reported in each graph's result too
+    auto fail = [&](vc_status st) {
+        for (uint32_t i = 0; i < count; ++i) {
+            out[i].status = st;
+            out[i].size = 0;
+            out[i].decision = 0;
+            out[i].has_cover = 0;
+            out[i].tree_nodes = 0;
+        }
+        return st;
+    };
     uint64_t rows = 0, cols = 0;
     for (uint32_t i = 0; i < count; ++i) {
-        if (reqs[i].instance != VC_MVC && reqs[i].instance != VC_PVC) return VC_ERR_INVALID;
-        if (a->n[i] > kMaxVertices) return VC_ERR_TOO_LARGE;
+        if (reqs[i].instance != VC_MVC && reqs[i].instance != VC_PVC) return fail(VC_ERR_INVALID);
+        if (a->n[i] > kMaxVertices) return fail(VC_ERR_TOO_LARGE);
         rows = std::max<uint64_t>(rows, a->row_off[i] + a->n[i] + 1);
     }
     for (uint32_t i = 0; i < count; ++i) {
@@ -585,12 +596,12 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
             g.col = a->col + a->col_off[i];
             g.degree = nullptr;
             vc_status v = validate_csr(&g);
-            if (v != VC_OK) return v;
+            if (v != VC_OK) return fail(v);
         }
     }
     vc_status err;
     Ctx *c = get_ctx(reqs[0].device, &err);
-    if (!c) return err;
+    if (!c) return fail(err);
     std::lock_guard<std::mutex> lk(c->mu);
     cudaStream_t stream = reqs[0].stream ? (cudaStream_t)reqs[0].stream : c->stream;
     Job job;
@@ -599,7 +610,7 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         job.d_col = d_col;
     } else {
         if (c->rp.ensure(sizeof(uint32_t) * rows) || c->col.ensure(sizeof(uint32_t) * std::max<uint64_t>(cols, 1)))
-            return VC_ERR_NOMEM;
+            return fail(VC_ERR_NOMEM);
         cudaMemcpyAsync(c->rp.p, a->row_ptr, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, stream);
         if (cols) cudaMemcpyAsync(c->col.p, a->col, sizeof(uint32_t) * cols, cudaMemcpyHostToDevice, stream);
         job.d_rp = (const uint32_t *)c->rp.p;

@@ -202,6 +202,12 @@ def batch_graphs(count: int = 4096, seed: int = 0, **kw) -> List[Graph]:
     return [batch_instance(i, seed, **kw) for i in range(count)]
 
 
+def rank_batch(count: int, rank: int) -> List[Graph]:
+    """The batch a rank of a multi-GPU run solves: the batched workload with the
+    rank as its seed (weak scaling: every rank has its own, disjoint graphs)."""
+    return batch_graphs(count, seed=rank)
+
+
 def stream_instance(i: int, seed: int = 0, n_lo: int = 50, n_hi: int = 5000) -> Graph:
     """Request i of the served stream: G(n, p) with average degree U[3, 12] or a
     random 3-regular graph (equal odds), n log-uniform in [n_lo, n_hi]."""

@@ -216,3 +216,18 @@ def test_csr_kernel_on_small_graphs():
     for g, r, rec in zip(graphs, sols, recs):
         _check_mvc(g, r, rec["opt"])
     assert single.status == vcgpu.VC_OK and single.decision == 0
+
+
+def test_time_limit_returns_timeout_and_device_stays_usable():
+    """A launch that reaches its time limit stops every search unit through its
+    bounded waits and reports VC_TIMEOUT; the next solve on the device works."""
+    recs = [r for r in _golden_batch(10**9) if r["nodes"] > 20_000_000]
+    g = W.batch_instance(recs[0]["i"])
+    r = vcgpu.solve(g, "mvc", time_limit=0.02)
+    assert r.status == vcgpu.VC_TIMEOUT
+    assert r.size >= recs[0]["opt"]
+    if r.cover is not None:
+        assert W.is_cover(g, r.cover) and int(r.cover.sum()) == r.size
+    g1 = W.config1_graph()
+    small = json.load(open(os.path.join(GOLDEN, "small.json")))
+    _check_mvc(g1, vcgpu.solve(g1, "mvc", time_limit=TL), small["config1"]["opt"])
