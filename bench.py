@@ -21,7 +21,14 @@ graph per launch ("plain") on a sample, for the batched-vs-plain ratio.
           bounded sample of the same graphs, all host cores
 
 `--impl reference` runs only the reference's CPU solver over bounded samples of
-the same workload (rank 0 only under torchrun).  Multi-GPU: every rank solves
+the same workload (rank 0 only under torchrun).
+
+`--workload stream` measures the served configuration instead: Poisson arrivals
+(default 2000 requests/s for 60 s), 70% MVC / 30% PVC with k = opt or opt-1,
+graphs drawn from the oracle-pinned pool of the stream family (G(n, p) and
+random 3-regular, n log-uniform in [50, 5000]; tests/golden/stream_seed0.jsonl),
+submitted to a vc_server as they arrive; it reports completed requests/s,
+p50/p99 latency from submission to completion, and checks every answer.  Multi-GPU: every rank solves
 its own batch (seed = rank): weak scaling, no collective on the data path.
 """
 from __future__ import annotations
@@ -59,6 +66,9 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=128)
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--ref-step-s", type=float, default=30.0)
+    ap.add_argument("--workload", default="batch", choices=["batch", "stream"])
+    ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--stream-seconds", type=float, default=60.0)
     return ap.parse_args()
 
 
@@ -343,12 +353,82 @@ def our_arm(args, world, rank, local, pg):
     print(json.dumps(line))
 
 
+def stream_arm(args, world, rank):
+    """The served stream through vc_server (rank 0; other ranks have no work)."""
+    if rank != 0:
+        return
+    import vcgpu
+    recs = [json.loads(l) for l in open(os.path.join(REPO, "tests", "golden", "stream_seed0.jsonl")) if l.strip()]
+    pinned = sorted([r for r in recs if r["status"] == "ok"], key=lambda r: r["i"])
+    pool = [(W.stream_instance(r["i"]), r["opt"]) for r in pinned]
+    rng = np.random.default_rng(1)
+    arrivals, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / args.rate))
+        if t > args.stream_seconds:
+            break
+        arrivals.append(t)
+    reqs = []
+    for a in arrivals:
+        g, opt = pool[int(rng.integers(len(pool)))]
+        if rng.random() < 0.7:
+            reqs.append((a, g, "mvc", 0, opt))
+        else:
+            reqs.append((a, g, "pvc", opt - int(rng.integers(0, 2)), opt))
+    max_n = max(g.n for g, _ in pool)
+    lat, bad, budget, done = [], 0, 0, 0
+    with vcgpu.Server(max_vertices=max_n, max_requests=4096, mem_budget=2 << 30) as srv:
+        for g, opt in pool[:32]:  # warm-up: kernel launch, first-touch of buffers
+            srv.wait(srv.submit(g, "mvc", node_limit=args.node_limit))
+        outstanding = {}
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(reqs) or outstanding:
+            now = time.perf_counter() - t0
+            while i < len(reqs) and reqs[i][0] <= now:
+                a, g, kind, k, opt = reqs[i]
+                outstanding[srv.submit(g, kind, k=k, node_limit=args.node_limit, validate=False)] = (g, kind, k, opt)
+                i += 1
+            for tk in list(outstanding):
+                r = srv.poll(tk, want_cover=False)
+                if r is None:
+                    continue
+                g, kind, k, opt = outstanding.pop(tk)
+                done += 1
+                lat.append(r.total_ms)
+                if r.status == vcgpu.VC_BUDGET:
+                    budget += 1
+                elif r.status != vcgpu.VC_OK:
+                    bad += 1
+                elif kind == "mvc" and r.size != opt:
+                    bad += 1
+                elif kind == "pvc" and r.decision != (1 if opt <= k else 0):
+                    bad += 1
+            if i < len(reqs) and not outstanding:
+                time.sleep(max(0.0, min(reqs[i][0] - (time.perf_counter() - t0), 0.001)))
+        wall = time.perf_counter() - t0
+    lat = np.asarray(lat)
+    line = {"metric": METRIC, "value": done / wall, "unit": "requests/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic",
+            "config": {"workload": f"served stream: Poisson {args.rate:.0f} req/s for {args.stream_seconds:.0f} s, "
+                                   "70% MVC / 30% PVC (k = opt or opt-1), G(n,p) and random 3-regular, "
+                                   "n log-uniform [50,5000], drawn from the oracle-pinned pool",
+                       "requests": len(reqs), "completed": done, "wrong": bad, "budget_exceeded": budget,
+                       "node_limit": args.node_limit, "pool": len(pool), "pool_coverage": len(pinned) / max(len(recs), 1),
+                       "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+                       "mean_latency_ms": float(lat.mean()), "max_vertices": max_n}}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":
             reference_arm(args, world, rank)
+        elif args.workload == "stream":
+            stream_arm(args, world, rank)
         else:
             our_arm(args, world, rank, local, pg)
     finally:

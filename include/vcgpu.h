@@ -127,7 +127,7 @@ vc_status vc_solve_batch_device(const vc_csr_arena *arena, const uint32_t *d_row
  * kernel admits requests while others run; graphs and search state stay on the
  * device.  mem_budget_bytes bounds the device arena holding admitted graphs
  * (0 = 1 GiB); max_requests is the number of device slots (0 = 1024);
- * max_vertices is the largest graph accepted (0 = 2048; <= 255 selects the
+ * max_vertices is the largest graph accepted (0 = 1024; <= 255 selects the
  * dense-bitset kernel).  A request is admitted when a slot and arena room for
  * its CSR are free.  submit validates and copies the graph and returns a
  * ticket; poll returns VC_PENDING until the ticket's result is ready, then

@@ -13,7 +13,10 @@
 namespace vch {
 
 // Search units are warps up to this vertex capacity, CTAs above it.
-constexpr uint32_t kWarpMaxNP = 2048;
+#ifndef VC_WARP_MAX_NP
+#define VC_WARP_MAX_NP 1024
+#endif
+constexpr uint32_t kWarpMaxNP = VC_WARP_MAX_NP;
 constexpr uint32_t kMaxVertices = 1u << 26;
 
 struct DevBuf {

@@ -161,7 +161,8 @@ struct BlockG {
 
 // ---------------------------------------------------------------- SU state
 // Workspace layout (bytes), np = vertex capacity, nw = np/32:
-//   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | aux[np] (np > 65536 only)
+//   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | cand[np] u32 |
+//   aux[np] (np > 65536 only)
 
 struct SUStat {
     unsigned long long passes, donations, donate_fail, receives, roots, busy, idle, polls, restored;
@@ -170,7 +171,7 @@ struct SUStat {
 struct SU {
     SUStat stat;
     int32_t *deg;
-    uint32_t *trail, *fpos, *fv, *marks, *bits, *ctr, *aux;
+    uint32_t *trail, *fpos, *fv, *marks, *bits, *ctr, *cand, *aux;
     // current graph
     const uint32_t *rp, *cl;
     uint32_t inst, n, nw, mode, k, cover_off;
@@ -192,7 +193,8 @@ __device__ __forceinline__ void su_bind(SU &s, uint8_t *ws, uint32_t np)
     s.marks = s.fv + np;
     s.bits = s.marks + nw;
     s.ctr = s.bits + nw;
-    s.aux = np > 65536u ? s.ctr + 4 : nullptr;
+    s.cand = s.ctr + 4;
+    s.aux = np > 65536u ? s.cand + np : nullptr;
 }
 
 __device__ __forceinline__ void mark(uint32_t *marks, uint32_t v) { atomicOr(&marks[v >> 5], 1u << (v & 31u)); }
@@ -229,7 +231,11 @@ struct ScanOut {
 };
 
 // One reduction pass.  Returns true if marks were found and applied (another
-// pass is needed); otherwise fills `o` with the fixpoint's statistics.
+// pass is needed); otherwise fills `o` with the fixpoint's statistics.  A first
+// sweep takes the statistics and the high-degree marks and gathers the degree-1/2
+// vertices into a list; the list is then worked one vertex per thread, so the
+// CSR row walks of the leaf and triangle rules run side by side instead of in
+// one divergent round per vertex slot.
 template <class G>
 __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound, ScanOut &o)
 {
@@ -245,7 +251,17 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
         if (ud + del >= bound) {  // high-degree rule (helperFunctions.cuh:323-327)
             mark(s.marks, v);
             marked = true;
-        } else if (d == 1) {      // degree-one rule (helperFunctions.cuh:252-265)
+        } else if (d <= 2) {
+            s.cand[atomicAdd(&s.ctr[1], 1u)] = v;
+        }
+    }
+    G::sync();
+    const uint32_t nc = s.ctr[1];
+    G::sync();
+    if (G::rank() == 0) s.ctr[1] = 0;
+    for (uint32_t i = G::rank(); i < nc; i += G::kSize) {
+        const uint32_t v = s.cand[i];
+        if (deg[v] == 1) {        // degree-one rule (helperFunctions.cuh:252-265)
             uint32_t e1 = __ldg(&s.rp[v + 1]);
             for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
                 uint32_t u = __ldg(&s.cl[e]);
@@ -255,7 +271,7 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
                     break;
                 }
             }
-        } else if (d == 2) {      // degree-two triangle rule (helperFunctions.cuh:384-417)
+        } else {                  // degree-two triangle rule (helperFunctions.cuh:384-417)
             uint32_t n1 = kNone, n2 = kNone;
             bool keep = false;
             uint32_t e1 = __ldg(&s.rp[v + 1]);
@@ -397,7 +413,7 @@ __device__ __forceinline__ void rebuild(SU &s)
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) pc += __popc(s.bits[w]);
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
     s.base_del = G::sum(pc);
-    if (G::rank() == 0) s.ctr[0] = 0;
+    if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; }
     G::sync();
 }
 
@@ -427,7 +443,7 @@ __device__ __forceinline__ void load_root(SU &s)
         s.deg[v] = v < s.n ? (int32_t)(__ldg(&s.rp[v + 1]) - __ldg(&s.rp[v])) : 0;
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
     s.base_del = 0;
-    if (G::rank() == 0) s.ctr[0] = 0;
+    if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; }
     G::sync();
 }
 

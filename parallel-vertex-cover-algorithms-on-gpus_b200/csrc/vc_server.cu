@@ -359,7 +359,7 @@ extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes,
     const uint64_t budget = mem_budget_bytes ? mem_budget_bytes : (1ull << 30);
     // the largest graph a request may have: it sizes the search units'
     // workspaces and picks the kernel (dense bitsets up to 255 vertices)
-    const uint32_t max_n = max_vertices ? max_vertices : 2048;
+    const uint32_t max_n = max_vertices ? max_vertices : 1024;
     if (max_n > kMaxVertices) { delete s; return VC_ERR_TOO_LARGE; }
     s->max_n = max_n;
     s->nw_max = (max_n + 31) / 32;

@@ -101,11 +101,12 @@ struct HostResult {
 };
 
 // Workspace layout (bytes), np = vertex capacity, nw = np/32:
-//   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | aux[np] (np > 65536 only)
+//   deg[np] int32 | trail[np] u32 | fpos[np] u32 | fv[np] u32 | marks[nw] | bits[nw] | ctr[4] | cand[np] u32 |
+//   aux[np] (np > 65536 only)
 VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
 {
     uint32_t nw = np / 32;
-    uint32_t b = 16u * np + 8u * nw + 16u;
+    uint32_t b = 20u * np + 8u * nw + 16u;
     if (np > 65536u) b += 4u * np;
     return (b + 15u) & ~15u;
 }
