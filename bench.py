@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--workload", default="batch", choices=["batch", "stream"])
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--stream-seconds", type=float, default=60.0)
+    ap.add_argument("--stream-max-vertices", type=int, default=0)
     return ap.parse_args()
 
 
@@ -359,7 +360,8 @@ def stream_arm(args, world, rank):
         return
     import vcgpu
     recs = [json.loads(l) for l in open(os.path.join(REPO, "tests", "golden", "stream_seed0.jsonl")) if l.strip()]
-    pinned = sorted([r for r in recs if r["status"] == "ok"], key=lambda r: r["i"])
+    pinned = sorted([r for r in recs if r["status"] == "ok" and
+                     (not args.stream_max_vertices or r["n"] <= args.stream_max_vertices)], key=lambda r: r["i"])
     pool = [(W.stream_instance(r["i"]), r["opt"]) for r in pinned]
     rng = np.random.default_rng(1)
     arrivals, t = [], 0.0
@@ -389,10 +391,8 @@ def stream_arm(args, world, rank):
                 a, g, kind, k, opt = reqs[i]
                 outstanding[srv.submit(g, kind, k=k, node_limit=args.node_limit, validate=False)] = (g, kind, k, opt)
                 i += 1
-            for tk in list(outstanding):
+            for tk in srv.completed():
                 r = srv.poll(tk, want_cover=False)
-                if r is None:
-                    continue
                 g, kind, k, opt = outstanding.pop(tk)
                 done += 1
                 lat.append(r.total_ms)
@@ -404,8 +404,8 @@ def stream_arm(args, world, rank):
                     bad += 1
                 elif kind == "pvc" and r.decision != (1 if opt <= k else 0):
                     bad += 1
-            if i < len(reqs) and not outstanding:
-                time.sleep(max(0.0, min(reqs[i][0] - (time.perf_counter() - t0), 0.001)))
+            nxt = reqs[i][0] - (time.perf_counter() - t0) if i < len(reqs) else 0.0005
+            time.sleep(max(0.0, min(nxt, 0.0005)))
         wall = time.perf_counter() - t0
     lat = np.asarray(lat)
     line = {"metric": METRIC, "value": done / wall, "unit": "requests/s", "n_gpus": 1, "steps": 1, "warmup": 1,

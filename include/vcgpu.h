@@ -139,6 +139,10 @@ vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t m
                            vc_server **out);
 vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket);
 vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out);
+/* Tickets finished since the last call and not yet collected by vc_server_poll
+ * (at most max_tickets, oldest first): lets a caller with many requests in
+ * flight poll only the finished ones. No counterpart in the reference. */
+vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32_t max_tickets, uint32_t *count);
 vc_status vc_server_destroy(vc_server *s);
 
 /* Solve one graph of at most 255 vertices without allocating any memory (no

@@ -78,6 +78,7 @@ struct vc_server {
     std::vector<SlotInfo> info;
     std::unordered_map<uint64_t, uint32_t> inflight;  // ticket -> slot
     std::unordered_map<uint64_t, Done> done;
+    std::deque<uint64_t> ready;  // finished tickets not yet reported by vc_server_completed
     uint64_t next_ticket = 1;
     uint64_t arena_bump = 0;
     uint64_t sub_tail = 0;
@@ -159,6 +160,7 @@ uint32_t admit(vc_server *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
         const uint64_t bytes = ((rows + cols) * 4 + 255) / 256 * 256;
         if (bytes > s->arena_cap) {  // can never fit
             s->done.emplace(p.ticket, Done{VC_ERR_NOMEM, 0, 0, 0, 0, 0.0f, {}});
+            s->ready.push_back(p.ticket);
             s->pending.pop_front();
             continue;
         }
@@ -251,6 +253,7 @@ uint32_t collect(vc_server *s)
         }
         d.total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - si.t_submit).count();
         s->done.emplace(kv.first, std::move(d));
+        s->ready.push_back(kv.first);
         finished.push_back(kv.first);
     }
     for (uint64_t t : finished) {
@@ -269,6 +272,7 @@ void fail_inflight(vc_server *s, vc_status st)
     for (auto &kv : s->inflight) {
         Done d{st, 0, 0, 0, 0, 0.0f, {}};
         s->done.emplace(kv.first, std::move(d));
+        s->ready.push_back(kv.first);
         s->free_slots.push_back(kv.second);
     }
     s->inflight.clear();
@@ -282,7 +286,10 @@ void request_loop(vc_server *s)
     while (true) {
         if (s->fatal != VC_OK) {
             fail_inflight(s, s->fatal);
-            for (auto &p : s->pending) s->done.emplace(p.ticket, Done{s->fatal, 0, 0, 0, 0, 0.0f, {}});
+            for (auto &p : s->pending) {
+                s->done.emplace(p.ticket, Done{s->fatal, 0, 0, 0, 0, 0.0f, {}});
+                s->ready.push_back(p.ticket);
+            }
             s->pending.clear();
             s->cv.notify_all();
             if (s->stop) break;
@@ -447,6 +454,20 @@ extern "C" vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *ou
     vc_status st = d.status;
     s->done.erase(it);
     return st;
+}
+
+extern "C" vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32_t max_tickets, uint32_t *count)
+{
+    if (!s || !count || (max_tickets && !tickets)) return VC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    uint32_t k = 0;
+    while (k < max_tickets && !s->ready.empty()) {
+        const uint64_t t = s->ready.front();
+        s->ready.pop_front();
+        if (s->done.count(t)) tickets[k++] = t;  // skip tickets already collected by vc_server_poll
+    }
+    *count = k;
+    return VC_OK;
 }
 
 extern "C" vc_status vc_server_destroy(vc_server *s)

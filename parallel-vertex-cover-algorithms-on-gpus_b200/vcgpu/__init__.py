@@ -105,6 +105,9 @@ def lib():
             L.vc_server_submit.restype = ctypes.c_int
             L.vc_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]
             L.vc_server_poll.restype = ctypes.c_int
+            L.vc_server_completed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                              ctypes.POINTER(ctypes.c_uint32)]
+            L.vc_server_completed.restype = ctypes.c_int
             L.vc_server_destroy.argtypes = [ctypes.c_void_p]
             L.vc_server_destroy.restype = ctypes.c_int
         _lib = L
@@ -270,6 +273,13 @@ class Server:
         if st == VC_ERR_INVALID:
             raise KeyError(ticket)
         return _solution(res, cover[:n] if cover is not None else None, n)
+
+    def completed(self, max_tickets: int = 4096) -> List[int]:
+        """Tickets that finished since the last call."""
+        buf = np.zeros(max_tickets, dtype=np.uint64)
+        cnt = ctypes.c_uint32(0)
+        lib().vc_server_completed(self._h, buf.ctypes.data, max_tickets, ctypes.byref(cnt))
+        return [int(x) for x in buf[:cnt.value]]
 
     def wait(self, ticket: int, timeout: float = 120.0, want_cover: bool = True) -> Solution:
         import time

@@ -112,3 +112,24 @@ def test_server_rejects_oversize():
     with vcgpu.Server(max_vertices=100) as srv:
         with pytest.raises(RuntimeError):
             srv.submit(W.gnp(150, 0.05, 1), "mvc")
+
+
+def test_server_completed_reports_each_ticket_once():
+    """vc_server_completed hands out every finished ticket exactly once and
+    never one that vc_server_poll already collected."""
+    mix = _mix(40, seed=11)
+    with vcgpu.Server(max_vertices=255) as srv:
+        first = srv.submit(mix[0][0], "mvc")
+        r0 = srv.wait(first)  # collected by poll before completed() sees it
+        _check(mix[0][0], r0, "mvc", 0, mix[0][1])
+        want = {srv.submit(g, "mvc"): (g, opt) for g, opt in mix[1:]}
+        seen = []
+        t0 = time.time()
+        while len(seen) < len(want) and time.time() - t0 < 60:
+            seen += srv.completed(max_tickets=7)
+            time.sleep(0.001)
+        assert sorted(seen) == sorted(want) and first not in seen
+        for t in seen:
+            g, opt = want[t]
+            _check(g, srv.poll(t), "mvc", 0, opt)
+        assert srv.completed() == []
