@@ -13,9 +13,13 @@
 //    words, uniform in every lane's registers, mirrored in shared memory); a
 //    vertex taken into the cover leaves L, so del = n - |L| and the cover is
 //    the complement of L;
-//  * deg(v) = popc(adj[v] & L), kept per vertex in a byte array (0xFF =
-//    removed); lane l owns vertices l, l+32, ...  After a pass takes a set M,
-//    only the words of M are re-counted;
+//  * deg(v) = popc(adj[v] & L), kept as bytes (0 = removed or isolated), four
+//    to a 32-bit word: lane l holds words l and l + 32 in registers, so the
+//    rule tests of a pass look at four vertices per instruction (SWAR byte
+//    arithmetic).  When a set M leaves L, only the rows of M are read: each
+//    lane subtracts the 4-bit slices of those rows that cover its vertices
+//    (the adjacency is symmetric).  After a backtrack the degrees are
+//    recounted, one vertex per lane;
 //  * the triangle test of a degree-2 vertex is one bit test and the leaf
 //    rule's neighbour one find-first-set: no serial CSR row walks;
 //  * backtracking: an undo trail of removed ids (u16) and frames of (trail
@@ -27,12 +31,23 @@
 
 namespace vcg {
 
-constexpr uint8_t kGone = 0xFFu;  // degs[] value of a removed vertex
-
 template <int NW>
 struct Rows {
     static constexpr int kStride = NW >= 8 ? NW + 4 : NW;  // dense_row_words
+    static constexpr int kJ = NW >= 8 ? 2 : 1;              // degree words per lane
 };
+
+// 0x80 in every byte of x that is zero, 0 elsewhere.
+__device__ __forceinline__ uint32_t bytes_zero(uint32_t x)
+{
+    return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);
+}
+
+// 4 bits -> the low bit of each of 4 bytes (bit b to bit 8b).
+__device__ __forceinline__ uint32_t spread4(uint32_t nib) { return (nib * 0x00204081u) & 0x01010101u; }
+
+// The top bits of 4 bytes (bit 8b+7) -> 4 bits (bit b).
+__device__ __forceinline__ uint32_t gather4(uint32_t hb) { return ((hb >> 7) * 0x01020408u) >> 24; }
 
 // extra CTA header words used by the dense kernel
 enum : uint32_t { kCpStaged = 5, kCpCursorClosed = 6 };
@@ -53,17 +68,22 @@ struct DSU {
     uint32_t *lsm;        // [NW] shared-memory mirror of L
     uint16_t *trail;      // [32*NW]
     uint16_t *cand;       // [32*NW] degree-1/2 vertices of the current pass
-    uint8_t *degs;        // [32*NW]
+    uint8_t *degs;        // [32*NW] staging copy of D for byte lookups
     uint32_t L[NW];
+    uint32_t D[Rows<NW>::kJ];   // degree bytes of vertices 4q..4q+3, q = 32j + lane
+    uint32_t Ln[Rows<NW>::kJ];  // their live bits (4 per word)
     const uint32_t *rp, *cl;
     uint32_t inst, n, nw, mode, k, cover_off;
     unsigned long long node_limit;
     uint32_t base_del, top;
     uint32_t c_best;
     uint32_t fr_bot, fr_top;
+    uint32_t pending;  // how the next node starts: kPendApply / kPendRecount with the set in marks
     unsigned long long local_nodes;
     unsigned long long deadline;
 };
+
+enum : uint32_t { kPendApply = 1, kPendRecount = 2 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
@@ -113,7 +133,20 @@ __device__ __forceinline__ void mirror_L(DSU<NW> &s)
     __syncwarp();
 }
 
-// Degrees of this lane's vertices from scratch (L mirrored in s.lsm).
+// The live bits of this lane's degree words (from the mirror of L).
+template <int NW>
+__device__ __forceinline__ void live_nibbles(DSU<NW> &s)
+{
+    const unsigned lane = lane_id();
+#pragma unroll
+    for (int j = 0; j < Rows<NW>::kJ; ++j) {
+        const uint32_t q = 32u * j + lane;
+        s.Ln[j] = q < 8u * s.nw ? (s.lsm[q >> 3] >> (4u * (lane & 7u))) & 0xFu : 0u;
+    }
+}
+
+// Degrees from scratch (L mirrored in s.lsm): one vertex per lane into the byte
+// staging array, then each lane picks up its words.
 template <int NW>
 __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
 {
@@ -122,18 +155,23 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
 #pragma unroll 1
     for (int k = 0; k < kmax; ++k) {
         const uint32_t v = lane + 32u * k;
-        uint8_t dv = kGone;
+        uint32_t c = 0;
         if (v < s.n && ((s.lsm[k] >> lane) & 1u)) {
             uint32_t r[NW];
             load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
-            uint32_t c = 0;
 #pragma unroll
             for (int w = 0; w < NW; ++w) c += __popc(r[w] & s.L[w]);
-            dv = (uint8_t)c;
         }
-        s.degs[v] = dv;
+        s.degs[v] = (uint8_t)c;
     }
     __syncwarp();
+    const uint32_t *d32 = reinterpret_cast<const uint32_t *>(s.degs);
+#pragma unroll
+    for (int j = 0; j < Rows<NW>::kJ; ++j) {
+        const uint32_t q = 32u * j + lane;
+        s.D[j] = q < 8u * s.nw ? d32[q] : 0u;
+    }
+    live_nibbles(s);
 }
 
 // Log the vertices of M on the trail (ascending) and drop them from L.
@@ -174,107 +212,127 @@ __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
     __syncwarp();
 }
 
-enum : int { kSweepKeep = 0, kSweepApply = 1, kSweepRecount = 2 };
-
-// One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh),
-// fused with the degree update it follows:
-//   kSweepRecount: degrees from scratch (after a pop, a received record, a root);
-//   kSweepApply:   the set M just left L (trail and L already updated):
-//                  subtract its edges from the live vertices, retire M;
-//   kSweepKeep:    degrees are current.
-// The same sweep takes the statistics and the high-degree marks and gathers the
-// degree-1/2 vertices with warp ballots; the gathered list is then worked one
-// vertex per lane.  Returns true if marks were made (left in s.marks).
+// The set in s.marks has just left L (trail, L and its mirror already
+// updated): subtract its edges from the degrees of the live vertices and zero
+// the bytes of the removed ones.
 template <int NW>
-__device__ __forceinline__ bool dense_pass(DSU<NW> &s, int mode, const uint32_t (&M)[NW], uint32_t del,
-                                           uint32_t bound, ScanOut &o)
+__device__ __forceinline__ void dense_apply(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
-    uint32_t sum = 0, maxd = 0, amax = kNone;
-    bool marked = false;
-    uint32_t ncand = 0;
-    const int kmax = (int)s.nw;
+    live_nibbles(s);
+    const uint32_t sh = 4u * (lane & 7u);
+    const uint32_t *rows = s.adj + (lane >> 3);  // word 4j + lane/8 of a row holds this lane's bits
 #pragma unroll 1
-    for (int k = 0; k < kmax; ++k) {
-        const uint32_t v = lane + 32u * k;
-        uint32_t dv = s.degs[v];
-        if (mode == kSweepRecount) {
-            if (v < s.n && ((s.lsm[k] >> lane) & 1u)) {
-                uint32_t r[NW];
-                load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
-                uint32_t c = 0;
+    for (uint32_t w = 0; w < s.nw; ++w) {
+        uint32_t m = s.marks[w];
+        while (m) {
+            const uint32_t u = 32u * w + (__ffs(m) - 1);
+            m &= m - 1;
+            const uint32_t *row = rows + u * Rows<NW>::kStride;
 #pragma unroll
-                for (int w = 0; w < NW; ++w) c += __popc(r[w] & s.L[w]);
-                dv = c;
-            } else {
-                dv = kGone;
-            }
-            s.degs[v] = (uint8_t)dv;
-        } else if (mode == kSweepApply && dv != kGone) {
-            if (!((s.lsm[k] >> lane) & 1u)) {
-                dv = kGone;
-                s.degs[v] = kGone;
-            } else if (dv != 0) {
-                uint32_t r[NW];
-                load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
-                uint32_t dec = 0;
-#pragma unroll
-                for (int w = 0; w < NW; ++w) dec += __popc(r[w] & M[w]);
-                if (dec) {
-                    dv -= dec;
-                    s.degs[v] = (uint8_t)dv;
-                }
-            }
+            for (int j = 0; j < Rows<NW>::kJ; ++j) s.D[j] -= spread4((row[4 * j] >> sh) & s.Ln[j]);
         }
-        bool cand = false;
-        if (dv != 0 && dv != kGone) {
-            sum += dv;
-            if (dv > maxd) { maxd = dv; amax = v; }
-            if (dv + del >= bound) {  // high-degree rule
-                atomicOr(&s.marks[k], 1u << lane);
-                marked = true;
-            } else {
-                cand = dv <= 2;
-            }
-        }
-        const uint32_t cm = __ballot_sync(0xffffffffu, cand);
-        if (cand) s.cand[ncand + __popc(cm & ((1u << lane) - 1u))] = (uint16_t)v;
-        ncand += __popc(cm);
     }
-    __syncwarp();
-    for (uint32_t i = lane; i < ncand; i += 32) {  // degree-one / degree-two triangle rules
-        const uint32_t v = s.cand[i];
-        const uint32_t dv = s.degs[v];
-        uint32_t r[NW];
-        load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
-        uint32_t n1 = kNone, n2 = kNone;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            uint32_t x = r[w] & s.L[w];
-            if (x && n2 == kNone) {
-                const uint32_t u = 32u * w + (__ffs(x) - 1);
-                if (n1 == kNone) {
-                    n1 = u;
-                    x &= x - 1;
-                    if (x) n2 = 32u * w + (__ffs(x) - 1);
-                } else {
-                    n2 = u;
-                }
+    for (int j = 0; j < Rows<NW>::kJ; ++j) s.D[j] &= spread4(s.Ln[j]) * 0xFFu;
+}
+
+// One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh)
+// on current degrees.  Byte tests over each lane's degree words find the
+// high-degree vertices (marked at once) and the degree-1/2 ones, which are
+// gathered into a list and worked one vertex per lane.  Returns true if marks
+// were made (left in s.marks); otherwise fills o with the degree sum, the
+// maximum degree and its lowest vertex.
+template <int NW>
+__device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
+{
+    constexpr int J = Rows<NW>::kJ;
+    const unsigned lane = lane_id();
+    const uint32_t sh = 4u * (lane & 7u);
+    const int tt = (int)bound - (int)del;  // the high-degree rule takes deg >= tt
+    const uint32_t tl = (uint32_t)(tt & 0x7F) * 0x01010101u;
+    bool marked = false;
+    uint32_t cn[J], ctot = 0;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const uint32_t d = s.D[j];
+        const uint32_t nz = ~bytes_zero(d) & 0x80808080u;
+        uint32_t ge;
+        if (tt <= 1) {
+            ge = nz;
+        } else if (tt > 255) {
+            ge = 0u;
+        } else {
+            const uint32_t lo = ((d | 0x80808080u) - tl) & 0x80808080u;  // low 7 bits >= tt's
+            ge = tt < 128 ? ((d & 0x80808080u) | lo) : (d & lo);
+        }
+        // degree 1 or 2: no bit above the low two, and exactly one of those set
+        const uint32_t d12 = bytes_zero(d & 0xFCFCFCFCu) & (((d ^ (d >> 1)) & 0x01010101u) << 7);
+        const uint32_t hn = gather4(ge);
+        if (hn) {
+            atomicOr(&s.marks[(32u * j + lane) >> 3], hn << sh);
+            marked = true;
+        }
+        cn[j] = gather4(d12 & ~ge);
+        ctot += __popc(cn[j]);
+    }
+    // compact the degree-1/2 candidates (at most 4J per lane) into s.cand
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t pre = 0, total = 0;
+#pragma unroll
+    for (int b = 0; b < (J == 2 ? 4 : 3); ++b) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
+        pre += __popc(bal & lt) << b;
+        total += __popc(bal) << b;
+    }
+    if (total) {
+        uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs);
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const uint32_t q = 32u * j + lane;
+            if (q < 8u * s.nw) d32[q] = s.D[j];
+            uint32_t m = cn[j];
+            while (m) {
+                const uint32_t b = __ffs(m) - 1;
+                m &= m - 1;
+                s.cand[pre++] = (uint16_t)(4u * q + b);
             }
         }
-        if (dv == 1) {
-            const uint32_t du = s.degs[n1];
-            if (du > 1 || n1 < v) {
-                atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
-                marked = true;
+        __syncwarp();
+        for (uint32_t i = lane; i < total; i += 32) {  // degree-one / degree-two triangle rules
+            const uint32_t v = s.cand[i];
+            const uint32_t dv = s.degs[v];
+            uint32_t r[NW];
+            load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+            uint32_t n1 = kNone, n2 = kNone;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                uint32_t x = r[w] & s.L[w];
+                if (x && n2 == kNone) {
+                    const uint32_t u = 32u * w + (__ffs(x) - 1);
+                    if (n1 == kNone) {
+                        n1 = u;
+                        x &= x - 1;
+                        if (x) n2 = 32u * w + (__ffs(x) - 1);
+                    } else {
+                        n2 = u;
+                    }
+                }
             }
-        } else if (n2 != kNone) {
-            const uint32_t d1 = s.degs[n1], d2 = s.degs[n2];
-            const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
-            if (!keep && ((s.adj[n2 * Rows<NW>::kStride + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
-                atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
-                atomicOr(&s.marks[n2 >> 5], 1u << (n2 & 31u));
-                marked = true;
+            if (dv == 1) {
+                const uint32_t du = s.degs[n1];
+                if (du > 1 || n1 < v) {
+                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                    marked = true;
+                }
+            } else if (n2 != kNone) {
+                const uint32_t d1 = s.degs[n1], d2 = s.degs[n2];
+                const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
+                if (!keep && ((s.adj[n2 * Rows<NW>::kStride + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
+                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                    atomicOr(&s.marks[n2 >> 5], 1u << (n2 & 31u));
+                    marked = true;
+                }
             }
         }
     }
@@ -283,28 +341,54 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, int mode, const uint32_t 
         __syncwarp();
         return true;
     }
-    o.sum = __reduce_add_sync(0xffffffffu, sum);
-    o.maxd = __reduce_max_sync(0xffffffffu, maxd);
-    o.amax = __reduce_min_sync(0xffffffffu, (maxd == o.maxd && maxd > 0) ? amax : kNone);
+    uint32_t acc = 0, mx = 0;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const uint32_t d = s.D[j];
+        acc += (d & 0x00FF00FFu) + ((d >> 8) & 0x00FF00FFu);
+        mx = max(mx, max(max(d & 0xFFu, (d >> 8) & 0xFFu), max((d >> 16) & 0xFFu, d >> 24)));
+    }
+    o.sum = __reduce_add_sync(0xffffffffu, (acc & 0xFFFFu) + (acc >> 16));
+    o.maxd = __reduce_max_sync(0xffffffffu, mx);
+    uint32_t first = kNone;
+    if (o.maxd > 0) {
+#pragma unroll
+        for (int j = J - 1; j >= 0; --j) {
+            const uint32_t e = bytes_zero(s.D[j] ^ (o.maxd * 0x01010101u));
+            if (e) first = 4u * (32u * j + lane) + ((__ffs(e) >> 3) - 1);
+        }
+    }
+    o.amax = __reduce_min_sync(0xffffffffu, first);
     return false;
 }
 
-// Reduction to a fixpoint, starting with the given sweep mode and pending set.
+// A node's settling: the pending set in s.marks leaves L and the degrees are
+// brought up to date (subtracted, or recounted after a backtrack or a new
+// record), then reduction passes run to a fixpoint, each pass's marks taking the
+// same path.  One copy of the push / update code serves every caller.
 template <int NW>
-__device__ __forceinline__ void dense_reduce(DSU<NW> &s, int mode, uint32_t (&M)[NW], uint32_t bound, ScanOut &o)
+__device__ __forceinline__ void dense_settle(DSU<NW> &s, uint32_t bound, ScanOut &o)
 {
     const unsigned lane = lane_id();
+    uint32_t how = s.pending;
+    s.pending = 0;
 #pragma unroll 1
     for (int pass = 0; pass < 4 * 32 * NW; ++pass) {
-        if (!dense_pass(s, mode, M, s.base_del + s.top, bound, o)) break;
-        const long long t0 = s.timed ? clock64() : 0;
+        if (how) {
+            const long long t0 = s.timed ? clock64() : 0;
+            uint32_t M[NW];
 #pragma unroll
-        for (int w = 0; w < NW; ++w) M[w] = s.marks[w];
-        __syncwarp();
-        if (lane < NW) s.marks[lane] = 0;
-        dense_push(s, M);
-        mode = kSweepApply;
-        if (s.timed) s.cyc.apply += (unsigned long long)(clock64() - t0);
+            for (int w = 0; w < NW; ++w) M[w] = s.marks[w];
+            dense_push(s, M);
+            if (how == kPendRecount) dense_degrees(s);
+            else dense_apply(s);
+            __syncwarp();
+            if (lane < NW) s.marks[lane] = 0;
+            __syncwarp();
+            if (s.timed) s.cyc.apply += (unsigned long long)(clock64() - t0);
+        }
+        if (!dense_pass(s, s.base_del + s.top, bound, o)) break;
+        how = kPendApply;
     }
 }
 
@@ -338,7 +422,7 @@ __device__ __forceinline__ void load_root(DSU<NW> &s)
     s.base_del = 0;
     if (lane_id() < NW) s.marks[lane_id()] = 0;
     mirror_L(s);
-    dense_degrees(s);
+    s.pending = kPendRecount;  // the node's settling counts the degrees
 }
 
 // From a received live bitmap in s.bits.
@@ -355,7 +439,7 @@ __device__ __forceinline__ void rebuild(DSU<NW> &s)
     s.base_del = s.n - live;
     if (lane_id() < NW) s.marks[lane_id()] = 0;
     mirror_L(s);
-    dense_degrees(s);
+    s.pending = kPendRecount;  // the node's settling counts the degrees
 }
 
 // The bottom frame's pending child as a live bitmap in s.bits: L at that frame
@@ -562,6 +646,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
     dsu_bind(s, ws, adj);
     s.inst = kNone;
     s.fr_bot = s.fr_top = 0;
+    s.pending = 0;
     s.local_nodes = 0;
     s.c_best = 0;
     s.top = 0;
@@ -576,10 +661,6 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
     uint32_t ticks = 0, c_flags = 0;
     unsigned long long c_state = 0;
     const unsigned lane = lane_id();
-    int sweep = kSweepKeep;  // how the next node's first pass brings degrees up to date
-    uint32_t pend[NW];       // the set that node's first pass subtracts (kSweepApply)
-#pragma unroll
-    for (int w = 0; w < NW; ++w) pend[w] = 0;
 
     for (;;) {
         if (!have) {
@@ -589,12 +670,10 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
                 const uint32_t f = s.frames[s.fr_top];
                 const uint32_t v = f & 0xffffu;
                 dense_restore(s, f >> 16);
-                uint32_t N[NW];
-                load_row<NW>(s.adj + v * Rows<NW>::kStride, N, NW);
-#pragma unroll
-                for (int w = 0; w < NW; ++w) N[w] &= s.L[w];
-                dense_push(s, N);
-                sweep = kSweepRecount;  // the child's first pass recounts
+                // L after the restore is its mirror plus the restored set in s.bits
+                if (lane < NW) s.marks[lane] = s.adj[v * Rows<NW>::kStride + lane] & (s.lsm[lane] | s.bits[lane]);
+                __syncwarp();
+                s.pending = kPendRecount;  // take N(v), then recount
                 have = true;
                 if (s.timed) s.cyc.pop += (unsigned long long)(clock64() - t_pop);
             } else {
@@ -605,8 +684,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
                 t_mark = clock64();
                 s.stat.idle += (unsigned long long)(t_mark - t0);
                 if (!got) break;
-                have = true;
-                sweep = kSweepKeep;  // load_root / rebuild counted the degrees
+                have = true;  // load_root / rebuild counted the degrees
                 ticks = 0;
             }
         }
@@ -631,6 +709,9 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         if (c_flags & (kFound | kBudget | kError)) {
             if (lane == 0 && !(c_flags & (kFound | kBudget))) atomicOr(&st.flags, kCut);
             s.fr_bot = s.fr_top = 0;
+            s.pending = 0;
+            if (lane < NW) s.marks[lane] = 0;
+            __syncwarp();
             have = false;
             continue;
         }
@@ -648,7 +729,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         ScanOut o = {0u, 0u, kNone};
         const long long t_scan = s.timed ? clock64() : 0;
         const unsigned long long apply0 = s.cyc.apply;
-        dense_reduce(s, sweep, pend, bound, o);
+        dense_settle(s, bound, o);
         if (s.timed) s.cyc.scan += (unsigned long long)(clock64() - t_scan) - (s.cyc.apply - apply0);
         const uint32_t del = s.base_del + s.top;
         const uint64_t edges = o.sum / 2;
@@ -686,10 +767,9 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         want = G::bcast(want);
         if (want == 1) donate_local<G, S>(s, P, cp);
         else if (want == 2 && donate_global<G, S>(s, P)) c_state += 1ull << 32;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) pend[w] = ((uint32_t)w == (v >> 5)) ? (1u << (v & 31u)) : 0u;
-        dense_push(s, pend);
-        sweep = kSweepApply;  // the child's first pass subtracts v's edges
+        if (lane == 0) s.marks[v >> 5] = 1u << (v & 31u);  // marks are clear after a settled node
+        __syncwarp();
+        s.pending = kPendApply;  // the child takes v
         if (s.timed) s.cyc.branch += (unsigned long long)(clock64() - t_br);
     }
     if (P.stats && lane == 0) {

@@ -7,7 +7,7 @@
 #include <mutex>
 #include <vector>
 
-#include "../../include/vcgpu.h"
+#include "vcgpu.h"
 #include "vc_types.h"
 
 namespace vch {

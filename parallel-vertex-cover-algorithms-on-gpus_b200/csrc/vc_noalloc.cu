@@ -28,7 +28,7 @@
 #include <mutex>
 
 #include "vc_dense.cuh"
-#include "../../include/vcgpu.h"
+#include "vcgpu.h"
 
 using namespace vcg;
 

@@ -19,7 +19,7 @@
 #include "vc_search.cuh"
 #include "vc_dense.cuh"
 #include "vc_host.h"
-#include "../../include/vcgpu.h"
+#include "vcgpu.h"
 
 using namespace vcg;
 
