@@ -53,17 +53,26 @@ __global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Param
     su_main<G>(P, ws, cp);
 }
 
-// Register budget of the dense search units (resident threads per SM).
+// Register budget of the dense search units (resident threads per SM): for
+// 8-word graphs 1280 (48 registers, five 256-thread CTAs) beat 1024 (64
+// registers) by 8% on the batched workload despite more spill traffic -- the
+// search is latency bound and more resident warps hide it; for 2/4-word graphs
+// 1536 (40 registers) measured best.
 #ifndef VC_DENSE8_THREADS
-#define VC_DENSE8_THREADS 1024
+#define VC_DENSE8_THREADS 1280
+#endif
+#ifndef VC_DENSE4_THREADS
+#define VC_DENSE4_THREADS 1536
 #endif
 template <int NW>
 struct DenseOcc {
-    static constexpr unsigned kThreads = NW >= 8 ? VC_DENSE8_THREADS : 1024;
+    static constexpr unsigned kThreads = NW >= 8 ? VC_DENSE8_THREADS : VC_DENSE4_THREADS;
+    template <unsigned NT>
+    static constexpr unsigned min_ctas() { return kThreads / NT < 32 ? kThreads / NT : 32; }  // 32 CTAs/SM at most
 };
 
 template <int NW, unsigned NT>
-__global__ void __launch_bounds__(NT, DenseOcc<NW>::kThreads / NT) k_dense(Params P)
+__global__ void __launch_bounds__(NT, DenseOcc<NW>::template min_ctas<NT>()) k_dense(Params P)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint32_t cp_hdr[kCpHdrWords];
