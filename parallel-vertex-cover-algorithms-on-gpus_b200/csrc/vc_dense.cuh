@@ -10,9 +10,9 @@
 //    by the CTA's warps, which split the graph's search tree among themselves
 //    through the CTA pool (vc_search.cuh);
 //  * one warp is one search unit; its node state is the live-vertex set L (NW
-//    words, uniform in every lane's registers, mirrored in shared memory); a
-//    vertex taken into the cover leaves L, so del = n - |L| and the cover is
-//    the complement of L;
+//    words in shared memory, word w kept by lane w; copied into registers
+//    where a whole row is masked with it); a vertex taken into the cover
+//    leaves L, so del = n - |L| and the cover is the complement of L;
 //  * deg(v) = popc(adj[v] & L), kept as bytes (0 = removed or isolated), four
 //    to a 32-bit word: lane l holds words l and l + 32 in registers, so the
 //    rule tests of a pass look at four vertices per instruction (SWAR byte
@@ -65,11 +65,10 @@ struct DSU {
     uint32_t *frames;     // [32*NW] (trail position << 16) | vertex
     uint32_t *marks;      // [NW]
     uint32_t *bits;       // [NW] record / scratch
-    uint32_t *lsm;        // [NW] shared-memory mirror of L
+    uint32_t *lsm;        // [NW] the live set L
     uint16_t *trail;      // [32*NW]
     uint16_t *cand;       // [32*NW] degree-1/2 vertices of the current pass
     uint8_t *degs;        // [32*NW] staging copy of D for byte lookups
-    uint32_t L[NW];
     uint32_t D[Rows<NW>::kJ];   // degree bytes of vertices 4q..4q+3, q = 32j + lane
     uint32_t Ln[Rows<NW>::kJ];  // their live bits (4 per word)
     const uint32_t *rp, *cl;
@@ -123,14 +122,11 @@ __device__ __forceinline__ void load_row(const uint32_t *row, uint32_t (&r)[NW],
     }
 }
 
+// All NW words of L into registers.
 template <int NW>
-__device__ __forceinline__ void mirror_L(DSU<NW> &s)
+__device__ __forceinline__ void load_L(const DSU<NW> &s, uint32_t (&L)[NW])
 {
-    const unsigned lane = lane_id();
-#pragma unroll
-    for (int w = 0; w < NW; ++w)
-        if (lane == (unsigned)w) s.lsm[w] = s.L[w];
-    __syncwarp();
+    load_row<NW>(s.lsm, L, NW);
 }
 
 // The live bits of this lane's degree words (from the mirror of L).
@@ -145,13 +141,15 @@ __device__ __forceinline__ void live_nibbles(DSU<NW> &s)
     }
 }
 
-// Degrees from scratch (L mirrored in s.lsm): one vertex per lane into the byte
-// staging array, then each lane picks up its words.
+// Degrees from scratch: one vertex per lane into the byte staging array, then
+// each lane picks up its words.
 template <int NW>
 __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
     const int kmax = (int)s.nw;
+    uint32_t L[NW];
+    load_L(s, L);
 #pragma unroll 1
     for (int k = 0; k < kmax; ++k) {
         const uint32_t v = lane + 32u * k;
@@ -160,7 +158,7 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
             uint32_t r[NW];
             load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
 #pragma unroll
-            for (int w = 0; w < NW; ++w) c += __popc(r[w] & s.L[w]);
+            for (int w = 0; w < NW; ++w) c += __popc(r[w] & L[w]);
         }
         s.degs[v] = (uint8_t)c;
     }
@@ -174,23 +172,29 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
     live_nibbles(s);
 }
 
-// Log the vertices of M on the trail (ascending) and drop them from L.
+// Log the vertices of the set in s.marks on the trail (ascending) and drop
+// them from L; lane w handles word w.
 template <int NW>
-__device__ __forceinline__ void dense_push(DSU<NW> &s, const uint32_t (&M)[NW])
+__device__ __forceinline__ void dense_push(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
-    uint32_t base = s.top;
+    const uint32_t mw = lane < NW ? s.marks[lane] : 0u;
+    const uint32_t c = __popc(mw);
+    uint32_t off = c;  // inclusive prefix over the words
 #pragma unroll
-    for (int w = 0; w < NW; ++w) {
-        const uint32_t m = M[w];
-        if (m) {
-            if ((m >> lane) & 1u) s.trail[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)(32u * w + lane);
-            base += __popc(m);
-        }
-        s.L[w] &= ~m;
+    for (int d = 1; d < NW; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, off, d);
+        if (lane >= (unsigned)d) off += t;
     }
-    s.top = base;
-    mirror_L(s);
+    const uint32_t total = __shfl_sync(0xffffffffu, off, NW - 1);
+    uint32_t pos = s.top + off - c, m = mw;
+    while (m) {
+        s.trail[pos++] = (uint16_t)(32u * lane + (__ffs(m) - 1));
+        m &= m - 1;
+    }
+    if (lane < NW) s.lsm[lane] &= ~mw;
+    s.top += total;
+    __syncwarp();
 }
 
 // Put the trail above `pos` back into L.
@@ -205,8 +209,7 @@ __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
         atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
     }
     __syncwarp();
-#pragma unroll
-    for (int w = 0; w < NW; ++w) s.L[w] |= s.bits[w];
+    if (lane < NW) s.lsm[lane] |= s.bits[lane];
     s.stat.restored += s.top - pos;
     s.top = pos;
     __syncwarp();
@@ -298,6 +301,8 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
                 s.cand[pre++] = (uint16_t)(4u * q + b);
             }
         }
+        uint32_t L[NW];
+        load_L(s, L);
         __syncwarp();
         for (uint32_t i = lane; i < total; i += 32) {  // degree-one / degree-two triangle rules
             const uint32_t v = s.cand[i];
@@ -307,7 +312,7 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
             uint32_t n1 = kNone, n2 = kNone;
 #pragma unroll
             for (int w = 0; w < NW; ++w) {
-                uint32_t x = r[w] & s.L[w];
+                uint32_t x = r[w] & L[w];
                 if (x && n2 == kNone) {
                     const uint32_t u = 32u * w + (__ffs(x) - 1);
                     if (n1 == kNone) {
@@ -376,10 +381,7 @@ __device__ __forceinline__ void dense_settle(DSU<NW> &s, uint32_t bound, ScanOut
     for (int pass = 0; pass < 4 * 32 * NW; ++pass) {
         if (how) {
             const long long t0 = s.timed ? clock64() : 0;
-            uint32_t M[NW];
-#pragma unroll
-            for (int w = 0; w < NW; ++w) M[w] = s.marks[w];
-            dense_push(s, M);
+            dense_push(s);
             if (how == kPendRecount) dense_degrees(s);
             else dense_apply(s);
             __syncwarp();
@@ -413,15 +415,15 @@ __device__ __forceinline__ void bind_graph(DSU<NW> &s, const Params &P, uint32_t
 template <class G, int NW>
 __device__ __forceinline__ void load_root(DSU<NW> &s)
 {
-#pragma unroll
-    for (int w = 0; w < NW; ++w) {
+    const unsigned w = lane_id();
+    if (w < NW) {
         const uint32_t lo = 32u * w;
-        s.L[w] = lo + 32u <= s.n ? 0xffffffffu : (lo < s.n ? (1u << (s.n - lo)) - 1u : 0u);
+        s.lsm[w] = lo + 32u <= s.n ? 0xffffffffu : (lo < s.n ? (1u << (s.n - lo)) - 1u : 0u);
+        s.marks[w] = 0;
     }
     s.top = 0;
     s.base_del = 0;
-    if (lane_id() < NW) s.marks[lane_id()] = 0;
-    mirror_L(s);
+    __syncwarp();
     s.pending = kPendRecount;  // the node's settling counts the degrees
 }
 
@@ -429,16 +431,16 @@ __device__ __forceinline__ void load_root(DSU<NW> &s)
 template <class G, int NW>
 __device__ __forceinline__ void rebuild(DSU<NW> &s)
 {
-    uint32_t live = 0;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) {
-        s.L[w] = (uint32_t)w < s.nw ? s.bits[w] : 0u;
-        live += __popc(s.L[w]);
+    const unsigned w = lane_id();
+    const uint32_t x = w < s.nw ? s.bits[w] : 0u;
+    if (w < NW) {
+        s.lsm[w] = x;
+        s.marks[w] = 0;
     }
+    const uint32_t live = __reduce_add_sync(0xffffffffu, __popc(x));
     s.top = 0;
     s.base_del = s.n - live;
-    if (lane_id() < NW) s.marks[lane_id()] = 0;
-    mirror_L(s);
+    __syncwarp();
     s.pending = kPendRecount;  // the node's settling counts the degrees
 }
 
@@ -670,8 +672,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
                 const uint32_t f = s.frames[s.fr_top];
                 const uint32_t v = f & 0xffffu;
                 dense_restore(s, f >> 16);
-                // L after the restore is its mirror plus the restored set in s.bits
-                if (lane < NW) s.marks[lane] = s.adj[v * Rows<NW>::kStride + lane] & (s.lsm[lane] | s.bits[lane]);
+                if (lane < NW) s.marks[lane] = s.adj[v * Rows<NW>::kStride + lane] & s.lsm[lane];
                 __syncwarp();
                 s.pending = kPendRecount;  // take N(v), then recount
                 have = true;
