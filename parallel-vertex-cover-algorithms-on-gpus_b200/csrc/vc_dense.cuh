@@ -221,23 +221,39 @@ __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
 template <int NW>
 __device__ __forceinline__ void dense_apply(DSU<NW> &s)
 {
+    constexpr int J = Rows<NW>::kJ;
     const unsigned lane = lane_id();
     live_nibbles(s);
     const uint32_t sh = 4u * (lane & 7u);
     const uint32_t *rows = s.adj + (lane >> 3);  // word 4j + lane/8 of a row holds this lane's bits
-#pragma unroll 1
-    for (uint32_t w = 0; w < s.nw; ++w) {
-        uint32_t m = s.marks[w];
-        while (m) {
-            const uint32_t u = 32u * w + (__ffs(m) - 1);
-            m &= m - 1;
-            const uint32_t *row = rows + u * Rows<NW>::kStride;
+    const uint32_t mw = lane < s.nw ? s.marks[lane] : 0u;  // lane w holds word w of the set
+    uint32_t wm = __ballot_sync(0xffffffffu, mw != 0u);
+    uint32_t acc[J];  // per-byte decrements (at most the degree, so no byte overflows)
 #pragma unroll
-            for (int j = 0; j < Rows<NW>::kJ; ++j) s.D[j] -= spread4((row[4 * j] >> sh) & s.Ln[j]);
+    for (int j = 0; j < J; ++j) acc[j] = 0u;
+    while (wm) {
+        const uint32_t w = __ffs(wm) - 1;
+        wm &= wm - 1;
+        uint32_t m = __shfl_sync(0xffffffffu, mw, w);
+        while (m) {  // two removed vertices per step
+            const uint32_t u1 = 32u * w + (__ffs(m) - 1);
+            m &= m - 1;
+            const uint32_t *r1 = rows + u1 * Rows<NW>::kStride;
+            if (m) {
+                const uint32_t u2 = 32u * w + (__ffs(m) - 1);
+                m &= m - 1;
+                const uint32_t *r2 = rows + u2 * Rows<NW>::kStride;
+#pragma unroll
+                for (int j = 0; j < J; ++j)
+                    acc[j] += spread4((r1[4 * j] >> sh) & s.Ln[j]) + spread4((r2[4 * j] >> sh) & s.Ln[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < J; ++j) acc[j] += spread4((r1[4 * j] >> sh) & s.Ln[j]);
+            }
         }
     }
 #pragma unroll
-    for (int j = 0; j < Rows<NW>::kJ; ++j) s.D[j] &= spread4(s.Ln[j]) * 0xFFu;
+    for (int j = 0; j < J; ++j) s.D[j] = (s.D[j] - acc[j]) & (spread4(s.Ln[j]) * 0xFFu);
 }
 
 // One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh)
