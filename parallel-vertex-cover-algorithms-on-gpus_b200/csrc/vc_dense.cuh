@@ -35,6 +35,7 @@ template <int NW>
 struct Rows {
     static constexpr int kStride = NW >= 8 ? NW + 4 : NW;  // dense_row_words
     static constexpr int kJ = NW >= 8 ? 2 : 1;              // degree words per lane
+    static constexpr int kTri = 32 * NW * kStride;          // offset of the triangle bitmap
 };
 
 // 0x80 in every byte of x that is zero, 0 elsewhere.
@@ -258,8 +259,9 @@ __device__ __forceinline__ void dense_apply(DSU<NW> &s)
 
 // One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh)
 // on current degrees.  Byte tests over each lane's degree words find the
-// high-degree vertices (marked at once) and the degree-1/2 ones, which are
-// gathered into a list and worked one vertex per lane.  Returns true if marks
+// high-degree vertices (marked at once) and the degree-1 ones and degree-2 ones
+// on a triangle of the graph, which are gathered into a list and worked one
+// vertex per lane.  Returns true if marks
 // were made (left in s.marks); otherwise fills o with the degree sum, the
 // maximum degree and its lowest vertex.
 template <int NW>
@@ -270,6 +272,7 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
     const uint32_t sh = 4u * (lane & 7u);
     const int tt = (int)bound - (int)del;  // the high-degree rule takes deg >= tt
     const uint32_t tl = (uint32_t)(tt & 0x7F) * 0x01010101u;
+    const uint32_t *tri = s.adj + Rows<NW>::kTri;
     bool marked = false;
     uint32_t cn[J], ctot = 0;
 #pragma unroll
@@ -285,8 +288,9 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
             const uint32_t lo = ((d | 0x80808080u) - tl) & 0x80808080u;  // low 7 bits >= tt's
             ge = tt < 128 ? ((d & 0x80808080u) | lo) : (d & lo);
         }
-        // degree 1 or 2: no bit above the low two, and exactly one of those set
-        const uint32_t d12 = bytes_zero(d & 0xFCFCFCFCu) & (((d ^ (d >> 1)) & 0x01010101u) << 7);
+        // degree 1, or degree 2 on a triangle of the graph
+        const uint32_t tn = (tri[(32u * j + lane) >> 3] >> sh) & 0xFu;
+        const uint32_t d12 = bytes_zero(d ^ 0x01010101u) | (bytes_zero(d ^ 0x02020202u) & (spread4(tn) << 7));
         const uint32_t hn = gather4(ge);
         if (hn) {
             atomicOr(&s.marks[(32u * j + lane) >> 3], hn << sh);
@@ -498,7 +502,7 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
     const unsigned lane = lane_id();
     const InstDesc d = load_desc(&P.inst[inst]);
     const uint32_t *rp = P.row_ptr + d.row_off, *cl = P.col + d.col_off;
-    for (uint32_t i = lane; i < 32u * NW * Rows<NW>::kStride; i += 32) adj[i] = 0;
+    for (uint32_t i = lane; i < Rows<NW>::kTri + 8u; i += 32) adj[i] = 0;
     __syncwarp();
     for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
         uint32_t *row = adj + v * Rows<NW>::kStride;
@@ -507,6 +511,28 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
             const uint32_t u = __ldcg(&cl[e]);
             row[u >> 5] |= 1u << (u & 31u);
         }
+    }
+    __syncwarp();
+    // tri: v has a neighbour u with a common neighbour.  Only such a vertex can
+    // ever meet the triangle rule (its two live neighbours adjacent), so the
+    // passes look at degree-2 vertices in tri only.
+    for (uint32_t v = lane; v < d.n; v += 32) {
+        uint32_t r[NW];
+        load_row<NW>(adj + v * Rows<NW>::kStride, r, NW);
+        bool t = false;
+#pragma unroll 1
+        for (uint32_t w = 0; w < (uint32_t)NW && !t; ++w) {
+            uint32_t x = adj[v * Rows<NW>::kStride + w];
+            while (x && !t) {
+                const uint32_t u = 32u * w + (__ffs(x) - 1);
+                x &= x - 1;
+                uint32_t c = 0;
+#pragma unroll
+                for (int k = 0; k < NW; ++k) c |= adj[u * Rows<NW>::kStride + k] & r[k];
+                t = c != 0u;
+            }
+        }
+        if (t) atomicOr(&adj[Rows<NW>::kTri + (v >> 5)], 1u << (v & 31u));
     }
     __threadfence_block();
     __syncwarp();

@@ -112,13 +112,14 @@ VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
 }
 
 // Dense-bitset search unit (graphs of at most 255 vertices, nw <= 8 words):
-// per CTA adj[32*nw][dense_row_words(nw)] u32; per warp
+// per CTA adj[32*nw][dense_row_words(nw)] u32, then tri[8] u32 (the vertices
+// that lie on a triangle of the staged graph); per warp
 //   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 |
 //   cand[32*nw] u16 | degs[32*nw] u8
 // Row stride in words: 8-word rows are padded to 12 so that the 16-byte row
 // loads of eight consecutive lanes fall in distinct shared-memory banks.
 VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw >= 8 ? nw + 4 : nw; }
-VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw); }
+VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw) + 32u; }
 VC_HD inline uint32_t dense_workspace_bytes(uint32_t nw)
 {
     uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 2u * 32u * nw + 32u * nw;
