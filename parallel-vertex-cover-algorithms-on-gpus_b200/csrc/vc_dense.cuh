@@ -53,6 +53,14 @@ __device__ __forceinline__ uint32_t gather4(uint32_t hb) { return ((hb >> 7) * 0
 // extra CTA header words used by the dense kernel
 enum : uint32_t { kCpStaged = 5, kCpCursorClosed = 6 };
 
+// Per-phase cycle counters of the statistics mode (vc_debug_stats) cost a
+// clock read and a branch per phase even when off, so they are compiled in
+// only with VC_PHASE_TIMERS=1.
+#ifndef VC_PHASE_TIMERS
+#define VC_PHASE_TIMERS 0
+#endif
+constexpr bool kPhaseTimers = VC_PHASE_TIMERS != 0;
+
 struct PhaseCycles {
     unsigned long long scan, apply, pop, branch;
 };
@@ -62,14 +70,15 @@ struct DSU {
     SUStat stat;
     PhaseCycles cyc;
     bool timed;
-    const uint32_t *adj;  // CTA-shared [32*NW][NW]
-    uint32_t *frames;     // [32*NW] (trail position << 16) | vertex
-    uint32_t *marks;      // [NW]
-    uint32_t *bits;       // [NW] record / scratch
-    uint32_t *lsm;        // [NW] the live set L
-    uint16_t *trail;      // [32*NW]
-    uint16_t *cand;       // [32*NW] degree-1/2 vertices of the current pass
-    uint8_t *degs;        // [32*NW] staging copy of D for byte lookups
+    const uint32_t *adj;  // CTA-shared [32*NW][kStride] rows, then the triangle bitmap
+    uint8_t *ws;          // this warp's workspace; the arrays below sit at fixed offsets
+    __device__ __forceinline__ uint32_t *frames() const { return reinterpret_cast<uint32_t *>(ws); }  // [32*NW] (trail position << 16) | vertex
+    __device__ __forceinline__ uint32_t *marks() const { return frames() + 32 * NW; }  // [NW]
+    __device__ __forceinline__ uint32_t *bits() const { return marks() + NW; }         // [NW] record / scratch
+    __device__ __forceinline__ uint32_t *lsm() const { return bits() + NW; }           // [NW] the live set L
+    __device__ __forceinline__ uint16_t *trail() const { return reinterpret_cast<uint16_t *>(lsm() + NW); }  // [32*NW]
+    __device__ __forceinline__ uint16_t *cand() const { return trail() + 32 * NW; }   // [32*NW] pass candidates
+    __device__ __forceinline__ uint8_t *degs() const { return reinterpret_cast<uint8_t *>(cand() + 32 * NW); }  // [32*NW] staging copy of D
     uint32_t D[Rows<NW>::kJ];   // degree bytes of vertices 4q..4q+3, q = 32j + lane
     uint32_t Ln[Rows<NW>::kJ];  // their live bits (4 per word)
     const uint32_t *rp, *cl;
@@ -91,14 +100,11 @@ template <int NW>
 __device__ __forceinline__ void dsu_bind(DSU<NW> &s, uint8_t *ws, const uint32_t *adj)
 {
     s.adj = adj;
-    s.frames = reinterpret_cast<uint32_t *>(ws);
-    s.marks = s.frames + 32 * NW;
-    s.bits = s.marks + NW;
-    s.lsm = s.bits + NW;
-    s.trail = reinterpret_cast<uint16_t *>(s.lsm + NW);
-    s.cand = s.trail + 32 * NW;
-    s.degs = reinterpret_cast<uint8_t *>(s.cand + 32 * NW);
+    s.ws = ws;
 }
+
+template <int NW>
+__device__ __forceinline__ uint32_t *rec_bits(DSU<NW> &s) { return s.bits(); }
 
 // Loads the first nw (runtime, uniform) words of a row; the rest read as 0.
 template <int NW>
@@ -127,7 +133,7 @@ __device__ __forceinline__ void load_row(const uint32_t *row, uint32_t (&r)[NW],
 template <int NW>
 __device__ __forceinline__ void load_L(const DSU<NW> &s, uint32_t (&L)[NW])
 {
-    load_row<NW>(s.lsm, L, NW);
+    load_row<NW>(s.lsm(), L, NW);
 }
 
 // The live bits of this lane's degree words (from the mirror of L).
@@ -138,7 +144,7 @@ __device__ __forceinline__ void live_nibbles(DSU<NW> &s)
 #pragma unroll
     for (int j = 0; j < Rows<NW>::kJ; ++j) {
         const uint32_t q = 32u * j + lane;
-        s.Ln[j] = q < 8u * s.nw ? (s.lsm[q >> 3] >> (4u * (lane & 7u))) & 0xFu : 0u;
+        s.Ln[j] = q < 8u * s.nw ? (s.lsm()[q >> 3] >> (4u * (lane & 7u))) & 0xFu : 0u;
     }
 }
 
@@ -155,16 +161,16 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
     for (int k = 0; k < kmax; ++k) {
         const uint32_t v = lane + 32u * k;
         uint32_t c = 0;
-        if (v < s.n && ((s.lsm[k] >> lane) & 1u)) {
+        if (v < s.n && ((s.lsm()[k] >> lane) & 1u)) {
             uint32_t r[NW];
             load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
 #pragma unroll
             for (int w = 0; w < NW; ++w) c += __popc(r[w] & L[w]);
         }
-        s.degs[v] = (uint8_t)c;
+        s.degs()[v] = (uint8_t)c;
     }
     __syncwarp();
-    const uint32_t *d32 = reinterpret_cast<const uint32_t *>(s.degs);
+    const uint32_t *d32 = reinterpret_cast<const uint32_t *>(s.degs());
 #pragma unroll
     for (int j = 0; j < Rows<NW>::kJ; ++j) {
         const uint32_t q = 32u * j + lane;
@@ -173,13 +179,13 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
     live_nibbles(s);
 }
 
-// Log the vertices of the set in s.marks on the trail (ascending) and drop
+// Log the vertices of the set in s.marks() on the trail (ascending) and drop
 // them from L; lane w handles word w.
 template <int NW>
 __device__ __forceinline__ void dense_push(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
-    const uint32_t mw = lane < NW ? s.marks[lane] : 0u;
+    const uint32_t mw = lane < NW ? s.marks()[lane] : 0u;
     const uint32_t c = __popc(mw);
     uint32_t off = c;  // inclusive prefix over the words
 #pragma unroll
@@ -190,10 +196,10 @@ __device__ __forceinline__ void dense_push(DSU<NW> &s)
     const uint32_t total = __shfl_sync(0xffffffffu, off, NW - 1);
     uint32_t pos = s.top + off - c, m = mw;
     while (m) {
-        s.trail[pos++] = (uint16_t)(32u * lane + (__ffs(m) - 1));
+        s.trail()[pos++] = (uint16_t)(32u * lane + (__ffs(m) - 1));
         m &= m - 1;
     }
-    if (lane < NW) s.lsm[lane] &= ~mw;
+    if (lane < NW) s.lsm()[lane] &= ~mw;
     s.top += total;
     __syncwarp();
 }
@@ -203,20 +209,20 @@ template <int NW>
 __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
 {
     const unsigned lane = lane_id();
-    if (lane < NW) s.bits[lane] = 0;
+    if (lane < NW) s.bits()[lane] = 0;
     __syncwarp();
     for (uint32_t i = pos + lane; i < s.top; i += 32) {
-        uint32_t u = s.trail[i];
-        atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
+        uint32_t u = s.trail()[i];
+        atomicOr(&s.bits()[u >> 5], 1u << (u & 31u));
     }
     __syncwarp();
-    if (lane < NW) s.lsm[lane] |= s.bits[lane];
+    if (lane < NW) s.lsm()[lane] |= s.bits()[lane];
     s.stat.restored += s.top - pos;
     s.top = pos;
     __syncwarp();
 }
 
-// The set in s.marks has just left L (trail, L and its mirror already
+// The set in s.marks() has just left L (trail, L and its mirror already
 // updated): subtract its edges from the degrees of the live vertices and zero
 // the bytes of the removed ones.
 template <int NW>
@@ -227,7 +233,7 @@ __device__ __forceinline__ void dense_apply(DSU<NW> &s)
     live_nibbles(s);
     const uint32_t sh = 4u * (lane & 7u);
     const uint32_t *rows = s.adj + (lane >> 3);  // word 4j + lane/8 of a row holds this lane's bits
-    const uint32_t mw = lane < s.nw ? s.marks[lane] : 0u;  // lane w holds word w of the set
+    const uint32_t mw = lane < s.nw ? s.marks()[lane] : 0u;  // lane w holds word w of the set
     uint32_t wm = __ballot_sync(0xffffffffu, mw != 0u);
     uint32_t acc[J];  // per-byte decrements (at most the degree, so no byte overflows)
 #pragma unroll
@@ -262,7 +268,7 @@ __device__ __forceinline__ void dense_apply(DSU<NW> &s)
 // high-degree vertices (marked at once) and the degree-1 ones and degree-2 ones
 // on a triangle of the graph, which are gathered into a list and worked one
 // vertex per lane.  Returns true if marks
-// were made (left in s.marks); otherwise fills o with the degree sum, the
+// were made (left in s.marks()); otherwise fills o with the degree sum, the
 // maximum degree and its lowest vertex.
 template <int NW>
 __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
@@ -279,27 +285,21 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
     for (int j = 0; j < J; ++j) {
         const uint32_t d = s.D[j];
         const uint32_t nz = ~bytes_zero(d) & 0x80808080u;
-        uint32_t ge;
-        if (tt <= 1) {
-            ge = nz;
-        } else if (tt > 255) {
-            ge = 0u;
-        } else {
-            const uint32_t lo = ((d | 0x80808080u) - tl) & 0x80808080u;  // low 7 bits >= tt's
-            ge = tt < 128 ? ((d & 0x80808080u) | lo) : (d & lo);
-        }
+        const uint32_t lo = ((d | 0x80808080u) - tl) & 0x80808080u;  // low 7 bits >= tt's
+        const uint32_t mid = tt < 128 ? ((d & 0x80808080u) | lo) : (d & lo);
+        const uint32_t ge = tt <= 1 ? nz : (tt > 255 ? 0u : mid);
         // degree 1, or degree 2 on a triangle of the graph
         const uint32_t tn = (tri[(32u * j + lane) >> 3] >> sh) & 0xFu;
         const uint32_t d12 = bytes_zero(d ^ 0x01010101u) | (bytes_zero(d ^ 0x02020202u) & (spread4(tn) << 7));
         const uint32_t hn = gather4(ge);
         if (hn) {
-            atomicOr(&s.marks[(32u * j + lane) >> 3], hn << sh);
+            atomicOr(&s.marks()[(32u * j + lane) >> 3], hn << sh);
             marked = true;
         }
         cn[j] = gather4(d12 & ~ge);
         ctot += __popc(cn[j]);
     }
-    // compact the degree-1/2 candidates (at most 4J per lane) into s.cand
+    // compact the degree-1/2 candidates (at most 4J per lane) into s.cand()
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t pre = 0, total = 0;
 #pragma unroll
@@ -309,7 +309,7 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
         total += __popc(bal) << b;
     }
     if (total) {
-        uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs);
+        uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs());
 #pragma unroll
         for (int j = 0; j < J; ++j) {
             const uint32_t q = 32u * j + lane;
@@ -318,44 +318,43 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
             while (m) {
                 const uint32_t b = __ffs(m) - 1;
                 m &= m - 1;
-                s.cand[pre++] = (uint16_t)(4u * q + b);
+                s.cand()[pre++] = (uint16_t)(4u * q + b);
             }
         }
         uint32_t L[NW];
         load_L(s, L);
         __syncwarp();
         for (uint32_t i = lane; i < total; i += 32) {  // degree-one / degree-two triangle rules
-            const uint32_t v = s.cand[i];
-            const uint32_t dv = s.degs[v];
+            const uint32_t v = s.cand()[i];
+            const uint32_t dv = s.degs()[v];
             uint32_t r[NW];
             load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
-            uint32_t n1 = kNone, n2 = kNone;
+            // v has exactly dv (1 or 2) live neighbours: the lowest and the
+            // highest set bit of row & L
+            uint32_t n1 = kNone, hi = kNone;
+#pragma unroll
+            for (int w = NW - 1; w >= 0; --w) {
+                const uint32_t x = r[w] & L[w];
+                n1 = x ? 32u * w + (__ffs(x) - 1) : n1;
+            }
 #pragma unroll
             for (int w = 0; w < NW; ++w) {
-                uint32_t x = r[w] & L[w];
-                if (x && n2 == kNone) {
-                    const uint32_t u = 32u * w + (__ffs(x) - 1);
-                    if (n1 == kNone) {
-                        n1 = u;
-                        x &= x - 1;
-                        if (x) n2 = 32u * w + (__ffs(x) - 1);
-                    } else {
-                        n2 = u;
-                    }
-                }
+                const uint32_t x = r[w] & L[w];
+                hi = x ? 32u * w + (31u - __clz(x)) : hi;
             }
+            const uint32_t n2 = dv == 2 ? hi : kNone;
             if (dv == 1) {
-                const uint32_t du = s.degs[n1];
+                const uint32_t du = s.degs()[n1];
                 if (du > 1 || n1 < v) {
-                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
+                    atomicOr(&s.marks()[n1 >> 5], 1u << (n1 & 31u));
                     marked = true;
                 }
             } else if (n2 != kNone) {
-                const uint32_t d1 = s.degs[n1], d2 = s.degs[n2];
+                const uint32_t d1 = s.degs()[n1], d2 = s.degs()[n2];
                 const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
                 if (!keep && ((s.adj[n2 * Rows<NW>::kStride + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
-                    atomicOr(&s.marks[n1 >> 5], 1u << (n1 & 31u));
-                    atomicOr(&s.marks[n2 >> 5], 1u << (n2 & 31u));
+                    atomicOr(&s.marks()[n1 >> 5], 1u << (n1 & 31u));
+                    atomicOr(&s.marks()[n2 >> 5], 1u << (n2 & 31u));
                     marked = true;
                 }
             }
@@ -387,7 +386,7 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
     return false;
 }
 
-// A node's settling: the pending set in s.marks leaves L and the degrees are
+// A node's settling: the pending set in s.marks() leaves L and the degrees are
 // brought up to date (subtracted, or recounted after a backtrack or a new
 // record), then reduction passes run to a fixpoint, each pass's marks taking the
 // same path.  One copy of the push / update code serves every caller.
@@ -400,14 +399,14 @@ __device__ __forceinline__ void dense_settle(DSU<NW> &s, uint32_t bound, ScanOut
 #pragma unroll 1
     for (int pass = 0; pass < 4 * 32 * NW; ++pass) {
         if (how) {
-            const long long t0 = s.timed ? clock64() : 0;
+            const long long t0 = (kPhaseTimers && s.timed) ? clock64() : 0;
             dense_push(s);
             if (how == kPendRecount) dense_degrees(s);
             else dense_apply(s);
             __syncwarp();
-            if (lane < NW) s.marks[lane] = 0;
+            if (lane < NW) s.marks()[lane] = 0;
             __syncwarp();
-            if (s.timed) s.cyc.apply += (unsigned long long)(clock64() - t0);
+            if (kPhaseTimers && s.timed) s.cyc.apply += (unsigned long long)(clock64() - t0);
         }
         if (!dense_pass(s, s.base_del + s.top, bound, o)) break;
         how = kPendApply;
@@ -438,8 +437,8 @@ __device__ __forceinline__ void load_root(DSU<NW> &s)
     const unsigned w = lane_id();
     if (w < NW) {
         const uint32_t lo = 32u * w;
-        s.lsm[w] = lo + 32u <= s.n ? 0xffffffffu : (lo < s.n ? (1u << (s.n - lo)) - 1u : 0u);
-        s.marks[w] = 0;
+        s.lsm()[w] = lo + 32u <= s.n ? 0xffffffffu : (lo < s.n ? (1u << (s.n - lo)) - 1u : 0u);
+        s.marks()[w] = 0;
     }
     s.top = 0;
     s.base_del = 0;
@@ -447,15 +446,15 @@ __device__ __forceinline__ void load_root(DSU<NW> &s)
     s.pending = kPendRecount;  // the node's settling counts the degrees
 }
 
-// From a received live bitmap in s.bits.
+// From a received live bitmap in s.bits().
 template <class G, int NW>
 __device__ __forceinline__ void rebuild(DSU<NW> &s)
 {
     const unsigned w = lane_id();
-    const uint32_t x = w < s.nw ? s.bits[w] : 0u;
+    const uint32_t x = w < s.nw ? s.bits()[w] : 0u;
     if (w < NW) {
-        s.lsm[w] = x;
-        s.marks[w] = 0;
+        s.lsm()[w] = x;
+        s.marks()[w] = 0;
     }
     const uint32_t live = __reduce_add_sync(0xffffffffu, __popc(x));
     s.top = 0;
@@ -464,22 +463,22 @@ __device__ __forceinline__ void rebuild(DSU<NW> &s)
     s.pending = kPendRecount;  // the node's settling counts the degrees
 }
 
-// The bottom frame's pending child as a live bitmap in s.bits: L at that frame
+// The bottom frame's pending child as a live bitmap in s.bits(): L at that frame
 // (L now plus the trail above the frame) minus N(v).
 template <class G, int NW>
 __device__ __forceinline__ void donation_bits(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
-    const uint32_t f = s.frames[s.fr_bot];
+    const uint32_t f = s.frames()[s.fr_bot];
     const uint32_t pos = f >> 16, v = f & 0xffffu;
-    if (lane < NW) s.bits[lane] = s.lsm[lane];
+    if (lane < NW) s.bits()[lane] = s.lsm()[lane];
     __syncwarp();
     for (uint32_t i = pos + lane; i < s.top; i += 32) {
-        uint32_t u = s.trail[i];
-        atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
+        uint32_t u = s.trail()[i];
+        atomicOr(&s.bits()[u >> 5], 1u << (u & 31u));
     }
     __syncwarp();
-    if (lane < NW) s.bits[lane] &= ~s.adj[v * Rows<NW>::kStride + lane];
+    if (lane < NW) s.bits()[lane] &= ~s.adj[v * Rows<NW>::kStride + lane];
     __syncwarp();
 }
 
@@ -490,7 +489,7 @@ __device__ __forceinline__ void cover_bits(DSU<NW> &s, uint32_t *dst)
     if (lane < s.nw) {
         const uint32_t lo = 32u * lane;
         const uint32_t valid = lo + 32u <= s.n ? 0xffffffffu : (1u << (s.n - lo)) - 1u;
-        dst[lane] = ~s.lsm[lane] & valid;
+        dst[lane] = ~s.lsm()[lane] & valid;
     }
 }
 
@@ -641,7 +640,7 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
             __threadfence_block();
             const uint32_t inst = vld(&d[0]);
             bind_graph<G>(s, P, inst);
-            for (uint32_t w = lane; w < s.nw; w += 32) s.bits[w] = vld(&d[4 + w]);
+            for (uint32_t w = lane; w < s.nw; w += 32) s.bits()[w] = vld(&d[4 + w]);
             __syncwarp();
             if (lane == 0) {
                 atomicSub(&cp.hdr[kCpCount], 1u);
@@ -665,7 +664,7 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
                 if (lane == 0) cp.hdr[kCpStaged] = key;
             }
             bind_graph<G>(s, P, inst);
-            for (uint32_t w = lane; w < s.nw; w += 32) s.bits[w] = __ldcg(&g[4 + w]);
+            for (uint32_t w = lane; w < s.nw; w += 32) s.bits()[w] = __ldcg(&g[4 + w]);
             __syncwarp();
             if (lane == 0) {
                 __threadfence();
@@ -709,16 +708,16 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
     for (;;) {
         if (!have) {
             if (s.inst != kNone && s.fr_top > s.fr_bot) {
-                const long long t_pop = s.timed ? clock64() : 0;
+                const long long t_pop = (kPhaseTimers && s.timed) ? clock64() : 0;
                 s.fr_top -= 1;
-                const uint32_t f = s.frames[s.fr_top];
+                const uint32_t f = s.frames()[s.fr_top];
                 const uint32_t v = f & 0xffffu;
                 dense_restore(s, f >> 16);
-                if (lane < NW) s.marks[lane] = s.adj[v * Rows<NW>::kStride + lane] & s.lsm[lane];
+                if (lane < NW) s.marks()[lane] = s.adj[v * Rows<NW>::kStride + lane] & s.lsm()[lane];
                 __syncwarp();
                 s.pending = kPendRecount;  // take N(v), then recount
                 have = true;
-                if (s.timed) s.cyc.pop += (unsigned long long)(clock64() - t_pop);
+                if (kPhaseTimers && s.timed) s.cyc.pop += (unsigned long long)(clock64() - t_pop);
             } else {
                 if (s.inst != kNone) finish_stint<G, S>(s, P);
                 long long t0 = clock64();
@@ -753,7 +752,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
             if (lane == 0 && !(c_flags & (kFound | kBudget))) atomicOr(&st.flags, kCut);
             s.fr_bot = s.fr_top = 0;
             s.pending = 0;
-            if (lane < NW) s.marks[lane] = 0;
+            if (lane < NW) s.marks()[lane] = 0;
             __syncwarp();
             have = false;
             continue;
@@ -770,10 +769,10 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         const uint32_t best = s.c_best;
         const uint32_t bound = s.mode == kModeMVC ? best : s.k + 1;
         ScanOut o = {0u, 0u, kNone};
-        const long long t_scan = s.timed ? clock64() : 0;
+        const long long t_scan = (kPhaseTimers && s.timed) ? clock64() : 0;
         const unsigned long long apply0 = s.cyc.apply;
         dense_settle(s, bound, o);
-        if (s.timed) s.cyc.scan += (unsigned long long)(clock64() - t_scan) - (s.cyc.apply - apply0);
+        if (kPhaseTimers && s.timed) s.cyc.scan += (unsigned long long)(clock64() - t_scan) - (s.cyc.apply - apply0);
         const uint32_t del = s.base_del + s.top;
         const uint64_t edges = o.sum / 2;
         bool prune;
@@ -796,9 +795,9 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
             have = false;
             continue;
         }
-        const long long t_br = s.timed ? clock64() : 0;
+        const long long t_br = (kPhaseTimers && s.timed) ? clock64() : 0;
         const uint32_t v = o.amax;
-        if (lane == 0) s.frames[s.fr_top] = (s.top << 16) | v;
+        if (lane == 0) s.frames()[s.fr_top] = (s.top << 16) | v;
         s.fr_top += 1;
         __syncwarp();
         uint32_t want = 0;
@@ -810,10 +809,10 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         want = G::bcast(want);
         if (want == 1) donate_local<G, S>(s, P, cp);
         else if (want == 2 && donate_global<G, S>(s, P)) c_state += 1ull << 32;
-        if (lane == 0) s.marks[v >> 5] = 1u << (v & 31u);  // marks are clear after a settled node
+        if (lane == 0) s.marks()[v >> 5] = 1u << (v & 31u);  // marks are clear after a settled node
         __syncwarp();
         s.pending = kPendApply;  // the child takes v
-        if (s.timed) s.cyc.branch += (unsigned long long)(clock64() - t_br);
+        if (kPhaseTimers && s.timed) s.cyc.branch += (unsigned long long)(clock64() - t_br);
     }
     if (P.stats && lane == 0) {
         unsigned long long *o = P.stats + (size_t)G::su_global() * kStatWords;

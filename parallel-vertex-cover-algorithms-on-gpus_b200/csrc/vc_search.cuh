@@ -183,6 +183,10 @@ struct SU {
     unsigned long long deadline;
 };
 
+// The record bitmap a search unit fills for donation (see donation_bits).
+__device__ __forceinline__ uint32_t *rec_bits(SU &s) { return s.bits; }
+
+
 __device__ __forceinline__ void su_bind(SU &s, uint8_t *ws, uint32_t np)
 {
     uint32_t nw = np / 32;
@@ -534,7 +538,7 @@ __device__ bool donate_local(S &s, const Params &P, CtaPool &cp)
         d[0] = s.inst;
         atomicAdd(&P.st[s.inst].act, 1u);
     }
-    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) d[4 + w] = s.bits[w];
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) d[4 + w] = rec_bits(s)[w];
     __threadfence_block();
     G::sync();
     if (G::rank() == 0) {
@@ -567,7 +571,7 @@ __device__ bool donate_global(S &s, const Params &P)
         atomicAdd(&P.st[s.inst].act, 1u);
         __stcg(&slot[0], s.inst);
     }
-    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) __stcg(&slot[4 + w], s.bits[w]);
+    for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) __stcg(&slot[4 + w], rec_bits(s)[w]);
     __threadfence();
     G::sync();
     if (G::rank() == 0) {
