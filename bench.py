@@ -380,6 +380,7 @@ def stream_arm(args, world, rank):
     max_n = max(g.n for g, _ in pool)
     lat, bad, budget, done = [], 0, 0, 0
     with vcgpu.Server(max_vertices=max_n, max_requests=4096, mem_budget=2 << 30) as srv:
+        lanes = srv.shape()
         for g, opt in pool[:32]:  # warm-up: kernel launch, first-touch of buffers
             srv.wait(srv.submit(g, "mvc", node_limit=args.node_limit))
         outstanding = {}
@@ -417,7 +418,7 @@ def stream_arm(args, world, rank):
                        "requests": len(reqs), "completed": done, "wrong": bad, "budget_exceeded": budget,
                        "node_limit": args.node_limit, "pool": len(pool), "pool_coverage": len(pinned) / max(len(recs), 1),
                        "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
-                       "mean_latency_ms": float(lat.mean()), "max_vertices": max_n}}
+                       "mean_latency_ms": float(lat.mean()), "max_vertices": max_n, "lanes": lanes}}
     print(json.dumps(line))
 
 

@@ -76,7 +76,12 @@ struct Job {
 };
 
 Ctx *get_ctx(int dev, vc_status *err);
-cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl);
+// smem_budget (bytes per CTA, 0 = the device limit) caps the CSR search units'
+// shared-memory workspaces; warp_max_np (0 = kWarpMaxNP) is the largest vertex
+// capacity given warp search units rather than 512-thread CTA units.
+cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, uint32_t smem_budget = 0,
+                      uint32_t warp_max_np = 0);
+void cap_plan(const Ctx &c, Plan &pl, uint32_t per_sm);
 vc_status run_job(Ctx &c, Job &job, cudaStream_t stream);
 vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out);
 vc_status validate_csr(const vc_csr *g);

@@ -1,8 +1,13 @@
 // vc_server.cu -- continuous-batching server (vc_server_* in include/vcgpu.h).
 //
-// One persistent search kernel per server runs on its own stream and keeps the
-// search state of every admitted request on the device.  A host thread (the
-// request loop):
+// A server has one or two lanes.  A lane is one persistent search kernel on its
+// own stream that keeps the search state of every admitted request on the
+// device.  When requests may exceed 255 vertices, small requests (the dense
+// bitset kernel, about three times the node rate) and large ones (the CSR
+// kernel) get a lane each; the two grids are sized so that both kernels are
+// resident side by side on every SM (3 dense CTAs per SM plus one CSR CTA in
+// the registers and shared memory left over), and neither kernel ever waits on
+// the other.  Each lane has a host thread (the request loop) that:
 //   * admits submitted requests into device slots while a slot and arena memory
 //     are free (admission by the request's device bytes: its CSR plus its cover
 //     bitmap; the search state itself lives in the kernel's fixed per-SU
@@ -59,7 +64,7 @@ constexpr uint32_t kSubQ = 1u << 16;  // submission queue entries (power of two)
 
 }  // namespace
 
-struct vc_server {
+struct SrvLane {
     int dev = -1;
     Ctx *ctx = nullptr;
     cudaStream_t kstream = nullptr, cstream = nullptr;
@@ -91,7 +96,7 @@ struct vc_server {
 
 namespace {
 
-vc_status launch_kernel(vc_server *s)
+vc_status launch_kernel(SrvLane *s)
 {
     // fresh control words, keeping the submission queue's head and tail
     unsigned long long ctl[kCtlWords];
@@ -148,7 +153,7 @@ vc_status launch_kernel(vc_server *s)
 // Admits pending requests into free slots (called by the loop, lock held):
 // copies their graphs and descriptors, then publishes their slot ids on the
 // submission queue with one synchronisation.  Returns the number admitted.
-uint32_t admit(vc_server *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
+uint32_t admit(SrvLane *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
 {
     arena_full = false;
     std::vector<Pending> batch;
@@ -220,7 +225,7 @@ uint32_t admit(vc_server *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
 }
 
 // Collects finished requests from the host-mapped records (lock held).
-uint32_t collect(vc_server *s)
+uint32_t collect(SrvLane *s)
 {
     uint32_t got = 0;
     std::vector<uint64_t> finished;
@@ -266,7 +271,7 @@ uint32_t collect(vc_server *s)
 }
 
 // After an abnormal kernel exit, requests still in flight get a timeout status.
-void fail_inflight(vc_server *s, vc_status st)
+void fail_inflight(SrvLane *s, vc_status st)
 {
     s->discard_queue = true;
     for (auto &kv : s->inflight) {
@@ -278,7 +283,7 @@ void fail_inflight(vc_server *s, vc_status st)
     s->inflight.clear();
 }
 
-void request_loop(vc_server *s)
+void request_loop(SrvLane *s)
 {
     cudaSetDevice(s->dev);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -349,130 +354,9 @@ void request_loop(vc_server *s)
     s->cv.notify_all();
 }
 
-}  // namespace
-
-extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests,
-                                     uint32_t max_vertices, vc_server **out)
+void lane_destroy(SrvLane *s)
 {
-    if (!out) return VC_ERR_INVALID;
-    *out = nullptr;
-    vc_status err;
-    Ctx *c = get_ctx(device, &err);
-    if (!c) return err;
-    vc_server *s = new vc_server();
-    s->dev = c->dev;
-    s->ctx = c;
-    s->slots = max_requests ? max_requests : 1024;
-    const uint64_t budget = mem_budget_bytes ? mem_budget_bytes : (1ull << 30);
-    // the largest graph a request may have: it sizes the search units'
-    // workspaces and picks the kernel (dense bitsets up to 255 vertices)
-    const uint32_t max_n = max_vertices ? max_vertices : 1024;
-    if (max_n > kMaxVertices) { delete s; return VC_ERR_TOO_LARGE; }
-    s->max_n = max_n;
-    s->nw_max = (max_n + 31) / 32;
-    if (make_plan(*c, std::max<uint32_t>(32, (max_n + 31) / 32 * 32), max_n, s->pl) != cudaSuccess) {
-        delete s;
-        return VC_ERR_CUDA;
-    }
-    s->q = 1024;
-    while (s->q < 2 * s->pl.num_su) s->q <<= 1;
-    s->res_words = (uint32_t)(sizeof(HostResult) / 4) + s->nw_max;
-    s->res_words = (s->res_words + 3) / 4 * 4;
-    s->arena_cap = budget;
-    bool ok = cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking) == cudaSuccess;
-    ok = ok && !s->desc.ensure(sizeof(InstDesc) * s->slots) && !s->st.ensure(sizeof(InstState) * s->slots) &&
-         !s->covers.ensure(4ull * s->slots * s->nw_max) && !s->ctl.ensure(sizeof(unsigned long long) * kCtlWords) &&
-         !s->seq.ensure(sizeof(unsigned long long) * s->q) && !s->data.ensure(4ull * s->q * s->pl.stride) &&
-         !s->subq.ensure(4ull * kSubQ) && !s->arena.ensure(budget) &&
-         (!s->pl.global_ws || !s->gws.ensure((size_t)s->pl.num_su * s->pl.su_bytes));
-    ok = ok && cudaMemset(s->ctl.p, 0, sizeof(unsigned long long) * kCtlWords) == cudaSuccess;
-    const size_t res_bytes = 4ull * s->slots * s->res_words;
-    ok = ok && cudaHostAlloc((void **)&s->h_res, res_bytes, cudaHostAllocMapped) == cudaSuccess;
-    ok = ok && cudaHostGetDevicePointer((void **)&s->d_res, s->h_res, 0) == cudaSuccess;
-    if (!ok) {
-        vc_server_destroy(s);
-        return VC_ERR_NOMEM;
-    }
-    memset(s->h_res, 0, res_bytes);
-    s->info.resize(s->slots);
-    for (uint32_t i = 0; i < s->slots; ++i) s->free_slots.push_back(s->slots - 1 - i);
-    s->loop = std::thread(request_loop, s);
-    *out = s;
-    return VC_OK;
-}
-
-extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket)
-{
-    if (!s || !g || !req || !ticket) return VC_ERR_INVALID;
-    if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
-    if (req->flags & VC_FLAG_DEVICE_INPUT) return VC_ERR_INVALID;  // the server copies from host memory
-    if (g->n == 0) return VC_ERR_INVALID;
-    if (g->n > s->max_n) return VC_ERR_TOO_LARGE;
-    if (!(req->flags & VC_FLAG_NO_VALIDATE)) {
-        vc_status v = validate_csr(g);
-        if (v != VC_OK) return v;
-    }
-    Pending p;
-    p.n = g->n;
-    p.m = g->m;
-    p.rp.assign(g->row_ptr, g->row_ptr + g->n + 1);
-    if (g->m) p.col.assign(g->col, g->col + 2ull * g->m);
-    p.req = *req;
-    p.t_submit = std::chrono::steady_clock::now();
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->stop) return VC_ERR_INVALID;
-    if (s->fatal != VC_OK) return s->fatal;
-    p.ticket = s->next_ticket++;
-    *ticket = p.ticket;
-    s->pending.push_back(std::move(p));
-    s->cv.notify_all();
-    return VC_OK;
-}
-
-extern "C" vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out)
-{
-    if (!s || !out) return VC_ERR_INVALID;
-    std::lock_guard<std::mutex> lk(s->mu);
-    auto it = s->done.find(ticket);
-    if (it == s->done.end()) {
-        if (s->inflight.count(ticket)) return VC_PENDING;
-        for (auto &p : s->pending)
-            if (p.ticket == ticket) return VC_PENDING;
-        return VC_ERR_INVALID;
-    }
-    Done &d = it->second;
-    out->status = d.status;
-    out->size = d.size;
-    out->decision = d.decision;
-    out->has_cover = d.has_cover;
-    out->tree_nodes = d.nodes;
-    out->kernel_ms = 0;
-    out->total_ms = d.total_ms;
-    out->done_ms = d.total_ms;
-    if (out->cover_mask && !d.cover.empty()) memcpy(out->cover_mask, d.cover.data(), d.cover.size());
-    vc_status st = d.status;
-    s->done.erase(it);
-    return st;
-}
-
-extern "C" vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32_t max_tickets, uint32_t *count)
-{
-    if (!s || !count || (max_tickets && !tickets)) return VC_ERR_INVALID;
-    std::lock_guard<std::mutex> lk(s->mu);
-    uint32_t k = 0;
-    while (k < max_tickets && !s->ready.empty()) {
-        const uint64_t t = s->ready.front();
-        s->ready.pop_front();
-        if (s->done.count(t)) tickets[k++] = t;  // skip tickets already collected by vc_server_poll
-    }
-    *count = k;
-    return VC_OK;
-}
-
-extern "C" vc_status vc_server_destroy(vc_server *s)
-{
-    if (!s) return VC_ERR_INVALID;
+    if (!s) return;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
@@ -491,6 +375,247 @@ extern "C" vc_status vc_server_destroy(vc_server *s)
     if (s->h_res) cudaFreeHost(s->h_res);
     if (s->kstream) cudaStreamDestroy(s->kstream);
     if (s->cstream) cudaStreamDestroy(s->cstream);
+    delete s;
+}
+
+// A lane for requests of at most max_n vertices with the given plan.
+vc_status lane_create(Ctx *c, uint64_t budget, uint32_t slots, uint32_t max_n, const Plan &pl, SrvLane **out)
+{
+    SrvLane *s = new SrvLane();
+    s->dev = c->dev;
+    s->ctx = c;
+    s->slots = slots;
+    s->max_n = max_n;
+    s->nw_max = (max_n + 31) / 32;
+    s->pl = pl;
+    s->q = 1024;
+    while (s->q < 2 * s->pl.num_su) s->q <<= 1;
+    s->res_words = (uint32_t)(sizeof(HostResult) / 4) + s->nw_max;
+    s->res_words = (s->res_words + 3) / 4 * 4;
+    s->arena_cap = budget;
+    bool ok = cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && !s->desc.ensure(sizeof(InstDesc) * s->slots) && !s->st.ensure(sizeof(InstState) * s->slots) &&
+         !s->covers.ensure(4ull * s->slots * s->nw_max) && !s->ctl.ensure(sizeof(unsigned long long) * kCtlWords) &&
+         !s->seq.ensure(sizeof(unsigned long long) * s->q) && !s->data.ensure(4ull * s->q * s->pl.stride) &&
+         !s->subq.ensure(4ull * kSubQ) && !s->arena.ensure(budget) &&
+         (!s->pl.global_ws || !s->gws.ensure((size_t)s->pl.num_su * s->pl.su_bytes));
+    ok = ok && cudaMemset(s->ctl.p, 0, sizeof(unsigned long long) * kCtlWords) == cudaSuccess;
+    const size_t res_bytes = 4ull * s->slots * s->res_words;
+    ok = ok && cudaHostAlloc((void **)&s->h_res, res_bytes, cudaHostAllocMapped) == cudaSuccess;
+    ok = ok && cudaHostGetDevicePointer((void **)&s->d_res, s->h_res, 0) == cudaSuccess;
+    if (!ok) {
+        lane_destroy(s);
+        return VC_ERR_NOMEM;
+    }
+    memset(s->h_res, 0, res_bytes);
+    s->info.resize(s->slots);
+    for (uint32_t i = 0; i < s->slots; ++i) s->free_slots.push_back(s->slots - 1 - i);
+    s->loop = std::thread(request_loop, s);
+    *out = s;
+    return VC_OK;
+}
+
+constexpr uint32_t kDenseMax = 255;       // the dense lane's largest request
+constexpr uint32_t kDenseCtasPerSm = 3;   // its CTAs per SM when it shares the device
+
+// Plans the two lanes so that kDenseCtasPerSm dense CTAs and one CSR CTA fit
+// on every SM together (registers, shared memory, warps, CTAs).  Returns false
+// when the CSR lane cannot fit beside the dense one.
+bool plan_split(Ctx &c, uint32_t max_n, Plan &pd, Plan &ps)
+{
+    if (make_plan(c, 32 * 8, kDenseMax, pd) != cudaSuccess || !pd.dense) return false;
+    int regs_sm = 0, smem_sm = 0, reserved = 0, warps_sm = 0, blocks_sm = 0;
+    if (cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&warps_sm, cudaDevAttrMaxThreadsPerMultiProcessor, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, c.dev) != cudaSuccess)
+        return false;
+    warps_sm /= 32;
+    cudaFuncAttributes fd;
+    if (cudaFuncGetAttributes(&fd, pd.fn) != cudaSuccess) return false;
+    auto warp_regs = [](int regs) { return (uint32_t)((regs * 32 + 255) / 256 * 256); };  // per-warp allocation
+    const uint32_t d_regs = kDenseCtasPerSm * (pd.block / 32) * warp_regs(fd.numRegs);
+    const uint32_t d_smem = kDenseCtasPerSm * (pd.smem + (uint32_t)fd.sharedSizeBytes + (uint32_t)reserved);
+    if (d_regs >= (uint32_t)regs_sm || d_smem + (uint32_t)reserved >= (uint32_t)smem_sm) return false;
+    const uint32_t smem_left = (uint32_t)smem_sm - d_smem - (uint32_t)reserved;
+    const uint32_t np = std::max<uint32_t>(32, (max_n + 31) / 32 * 32);
+    // warp units for the CSR lane at any size whose workspace fits beside the
+    // dense CTAs: more units than one 512-thread CTA per SM
+    if (make_plan(c, np, max_n, ps, smem_left, 1u << 16) != cudaSuccess || ps.dense) return false;
+    cudaFuncAttributes fs;
+    if (cudaFuncGetAttributes(&fs, ps.fn) != cudaSuccess) return false;
+    const bool fits = d_regs + (ps.block / 32) * warp_regs(fs.numRegs) <= (uint32_t)regs_sm &&
+                      d_smem + ps.smem + (uint32_t)fs.sharedSizeBytes + (uint32_t)reserved <= (uint32_t)smem_sm &&
+                      kDenseCtasPerSm * (pd.block / 32) + ps.block / 32 <= (uint32_t)warps_sm &&
+                      kDenseCtasPerSm + 1 <= (uint32_t)blocks_sm;
+    if (!fits) return false;
+    cap_plan(c, pd, kDenseCtasPerSm);
+    cap_plan(c, ps, 1);
+    return true;
+}
+
+}  // namespace
+
+// Public handle: the lanes; a ticket carries its lane in the low bit.
+struct vc_server {
+    std::vector<SrvLane *> lanes;
+    uint32_t max_n = 0;
+};
+
+namespace {
+inline SrvLane *lane_of(vc_server *s, uint64_t ticket, uint64_t *lt)
+{
+    const uint32_t li = (uint32_t)(ticket & 1u);
+    if (li >= s->lanes.size()) return nullptr;
+    *lt = ticket >> 1;
+    return s->lanes[li];
+}
+}  // namespace
+
+extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests,
+                                     uint32_t max_vertices, vc_server **out)
+{
+    if (!out) return VC_ERR_INVALID;
+    *out = nullptr;
+    vc_status err;
+    Ctx *c = get_ctx(device, &err);
+    if (!c) return err;
+    const uint32_t slots = max_requests ? max_requests : 1024;
+    const uint64_t budget = mem_budget_bytes ? mem_budget_bytes : (1ull << 30);
+    // the largest graph a request may have: it sizes the search units'
+    // workspaces and picks the kernels (dense bitsets up to 255 vertices)
+    const uint32_t max_n = max_vertices ? max_vertices : 1024;
+    if (max_n > kMaxVertices) return VC_ERR_TOO_LARGE;
+    vc_server *s = new vc_server();
+    s->max_n = max_n;
+    Plan pd, ps;
+    if (max_n > kDenseMax && !c->force_sparse && plan_split(*c, max_n, pd, ps)) {
+        SrvLane *a = nullptr, *b = nullptr;
+        vc_status e = lane_create(c, budget / 2, slots, kDenseMax, pd, &a);
+        if (e == VC_OK) e = lane_create(c, budget - budget / 2, slots, max_n, ps, &b);
+        if (e != VC_OK) {
+            lane_destroy(a);
+            delete s;
+            return e;
+        }
+        s->lanes = {a, b};
+    } else {
+        Plan pl;
+        if (make_plan(*c, std::max<uint32_t>(32, (max_n + 31) / 32 * 32), max_n, pl) != cudaSuccess) {
+            delete s;
+            return VC_ERR_CUDA;
+        }
+        SrvLane *a = nullptr;
+        vc_status e = lane_create(c, budget, slots, max_n, pl, &a);
+        if (e != VC_OK) {
+            delete s;
+            return e;
+        }
+        s->lanes = {a};
+    }
+    *out = s;
+    return VC_OK;
+}
+
+extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket)
+{
+    if (!s || !g || !req || !ticket) return VC_ERR_INVALID;
+    if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
+    if (req->flags & VC_FLAG_DEVICE_INPUT) return VC_ERR_INVALID;  // the server copies from host memory
+    if (g->n == 0) return VC_ERR_INVALID;
+    if (g->n > s->max_n) return VC_ERR_TOO_LARGE;
+    if (!(req->flags & VC_FLAG_NO_VALIDATE)) {
+        vc_status v = validate_csr(g);
+        if (v != VC_OK) return v;
+    }
+    const uint32_t li = (s->lanes.size() > 1 && g->n <= kDenseMax) ? 0u : (uint32_t)s->lanes.size() - 1u;
+    SrvLane *l = s->lanes[li];
+    Pending p;
+    p.n = g->n;
+    p.m = g->m;
+    p.rp.assign(g->row_ptr, g->row_ptr + g->n + 1);
+    if (g->m) p.col.assign(g->col, g->col + 2ull * g->m);
+    p.req = *req;
+    p.t_submit = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lk(l->mu);
+    if (l->stop) return VC_ERR_INVALID;
+    if (l->fatal != VC_OK) return l->fatal;
+    p.ticket = l->next_ticket++;
+    *ticket = (p.ticket << 1) | li;
+    l->pending.push_back(std::move(p));
+    l->cv.notify_all();
+    return VC_OK;
+}
+
+extern "C" vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out)
+{
+    if (!s || !out) return VC_ERR_INVALID;
+    uint64_t lt = 0;
+    SrvLane *l = lane_of(s, ticket, &lt);
+    if (!l) return VC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(l->mu);
+    auto it = l->done.find(lt);
+    if (it == l->done.end()) {
+        if (l->inflight.count(lt)) return VC_PENDING;
+        for (auto &p : l->pending)
+            if (p.ticket == lt) return VC_PENDING;
+        return VC_ERR_INVALID;
+    }
+    Done &d = it->second;
+    out->status = d.status;
+    out->size = d.size;
+    out->decision = d.decision;
+    out->has_cover = d.has_cover;
+    out->tree_nodes = d.nodes;
+    out->kernel_ms = 0;
+    out->total_ms = d.total_ms;
+    out->done_ms = d.total_ms;
+    if (out->cover_mask && !d.cover.empty()) memcpy(out->cover_mask, d.cover.data(), d.cover.size());
+    vc_status st = d.status;
+    l->done.erase(it);
+    return st;
+}
+
+extern "C" vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32_t max_tickets, uint32_t *count)
+{
+    if (!s || !count || (max_tickets && !tickets)) return VC_ERR_INVALID;
+    uint32_t k = 0;
+    for (uint32_t li = 0; li < s->lanes.size(); ++li) {
+        SrvLane *l = s->lanes[li];
+        std::lock_guard<std::mutex> lk(l->mu);
+        while (k < max_tickets && !l->ready.empty()) {
+            const uint64_t t = l->ready.front();
+            l->ready.pop_front();
+            if (l->done.count(t)) tickets[k++] = (t << 1) | li;  // skip tickets already collected by vc_server_poll
+        }
+    }
+    *count = k;
+    return VC_OK;
+}
+
+extern "C" vc_status vc_server_shape(vc_server *s, uint32_t *shape, uint32_t max_lanes, uint32_t *lanes)
+{
+    if (!s || !lanes || (max_lanes && !shape)) return VC_ERR_INVALID;
+    *lanes = (uint32_t)s->lanes.size();
+    for (uint32_t i = 0; i < s->lanes.size() && i < max_lanes; ++i) {
+        const SrvLane *l = s->lanes[i];
+        uint32_t *o = shape + 6 * i;
+        o[0] = l->max_n;
+        o[1] = l->pl.grid;
+        o[2] = l->pl.block;
+        o[3] = l->pl.num_su;
+        o[4] = l->pl.smem;
+        o[5] = l->pl.dense ? 1u : 0u;
+    }
+    return VC_OK;
+}
+
+extern "C" vc_status vc_server_destroy(vc_server *s)
+{
+    if (!s) return VC_ERR_INVALID;
+    for (SrvLane *l : s->lanes) lane_destroy(l);
     delete s;
     return VC_OK;
 }

@@ -254,7 +254,7 @@ static cudaError_t plan_dense(Ctx &c, Plan &pl)
     return cudaSuccess;
 }
 
-cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl)
+cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, uint32_t smem_budget, uint32_t warp_max_np)
 {
     pl.dense = false;
     // dense bitsets up to 255 vertices (degrees are bytes, 0xFF marks a removed vertex)
@@ -265,8 +265,9 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl)
     pl.su_bytes = su_workspace_bytes(np);
     pl.stride = (4 + np / 32 + 3) / 4 * 4;
     const uint32_t static_smem = 1024;  // reductions / broadcasts / CTA pool header
-    const uint32_t budget = (uint32_t)c.smem_optin - static_smem;
-    if (np <= kWarpMaxNP) {
+    uint32_t budget = (uint32_t)c.smem_optin - static_smem;
+    if (smem_budget) budget = std::min(budget, smem_budget > static_smem ? smem_budget - static_smem : 0u);
+    if (np <= (warp_max_np ? warp_max_np : kWarpMaxNP)) {
         uint32_t warps = 8;
         while (warps > 1 && warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget) warps >>= 1;
         if (warps * pl.su_bytes + cta_pool_bytes(warps > 1 ? 2 * warps : 0, pl.stride) <= budget) {
@@ -297,6 +298,15 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl)
     }
     pl.num_su = pl.grid;
     return cudaSuccess;
+}
+
+// Caps a plan's persistent grid at `per_sm` CTAs per SM (a server lane that
+// shares the device with another lane's kernel).
+void cap_plan(const Ctx &c, Plan &pl, uint32_t per_sm)
+{
+    const uint32_t su_per_cta = pl.grid ? pl.num_su / pl.grid : 1;
+    pl.grid = std::min(pl.grid, per_sm * (uint32_t)c.sms);
+    pl.num_su = pl.grid * su_per_cta;
 }
 
 // ---------------------------------------------------------------- one launch

@@ -108,6 +108,9 @@ def lib():
             L.vc_server_completed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                               ctypes.POINTER(ctypes.c_uint32)]
             L.vc_server_completed.restype = ctypes.c_int
+            L.vc_server_shape.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                          ctypes.POINTER(ctypes.c_uint32)]
+            L.vc_server_shape.restype = ctypes.c_int
             L.vc_server_destroy.argtypes = [ctypes.c_void_p]
             L.vc_server_destroy.restype = ctypes.c_int
         _lib = L
@@ -280,6 +283,16 @@ class Server:
         cnt = ctypes.c_uint32(0)
         lib().vc_server_completed(self._h, buf.ctypes.data, max_tickets, ctypes.byref(cnt))
         return [int(x) for x in buf[:cnt.value]]
+
+    def shape(self) -> List[dict]:
+        """The server's lanes: largest request, grid, block, search units, shared
+        memory per CTA and kernel kind."""
+        buf = np.zeros(12, dtype=np.uint32)
+        cnt = ctypes.c_uint32(0)
+        lib().vc_server_shape(self._h, buf.ctypes.data, 2, ctypes.byref(cnt))
+        return [{"max_vertices": int(buf[6 * i]), "grid": int(buf[6 * i + 1]), "block": int(buf[6 * i + 2]),
+                 "search_units": int(buf[6 * i + 3]), "smem_bytes": int(buf[6 * i + 4]),
+                 "kernel": "dense" if buf[6 * i + 5] else "csr"} for i in range(min(int(cnt.value), 2))]
 
     def wait(self, ticket: int, timeout: float = 120.0, want_cover: bool = True) -> Solution:
         import time

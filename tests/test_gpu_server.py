@@ -133,3 +133,27 @@ def test_server_completed_reports_each_ticket_once():
             g, opt = want[t]
             _check(g, srv.poll(t), "mvc", 0, opt)
         assert srv.completed() == []
+
+
+def test_server_two_lanes_small_and_large():
+    """With max_vertices above 255 the server runs a dense lane for small
+    requests and a CSR lane for large ones side by side; results match the
+    oracle-pinned optima alone and in a mix, and both lanes take requests."""
+    recs = [json.loads(l) for l in open(os.path.join(GOLDEN, "stream_seed0.jsonl"))]
+    pinned = sorted([r for r in recs if r["status"] == "ok" and r["nodes"] <= 300_000], key=lambda r: r["i"])
+    large = [r for r in pinned if r["n"] > 255][:6]
+    small = [r for r in pinned if r["n"] <= 255][:18]
+    assert large and small
+    items = [(W.stream_instance(r["i"]), r["opt"]) for r in large + small]
+    max_n = max(g.n for g, _ in items)
+    with vcgpu.Server(max_vertices=max_n) as srv:
+        g0, o0 = items[0]
+        _check(g0, srv.wait(srv.submit(g0, "mvc")), "mvc", 0, o0)  # a large one alone
+        tickets = [srv.submit(g, "mvc") for g, _ in items]
+        tickets += [srv.submit(g, "pvc", k=opt - 1) for g, opt in items[::3]]
+        res = [srv.wait(t) for t in tickets]
+    assert {t & 1 for t in tickets} == {0, 1}
+    for (g, opt), r in zip(items, res):
+        _check(g, r, "mvc", 0, opt)
+    for (g, opt), r in zip(items[::3], res[len(items):]):
+        _check(g, r, "pvc", opt - 1, opt)
