@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--stream-seconds", type=float, default=60.0)
     ap.add_argument("--stream-max-vertices", type=int, default=0)
+    ap.add_argument("--stream-min-vertices", type=int, default=0)
     return ap.parse_args()
 
 
@@ -360,7 +361,7 @@ def stream_arm(args, world, rank):
         return
     import vcgpu
     recs = [json.loads(l) for l in open(os.path.join(REPO, "tests", "golden", "stream_seed0.jsonl")) if l.strip()]
-    pinned = sorted([r for r in recs if r["status"] == "ok" and
+    pinned = sorted([r for r in recs if r["status"] == "ok" and r["n"] >= args.stream_min_vertices and
                      (not args.stream_max_vertices or r["n"] <= args.stream_max_vertices)], key=lambda r: r["i"])
     pool = [(W.stream_instance(r["i"]), r["opt"]) for r in pinned]
     rng = np.random.default_rng(1)
@@ -379,6 +380,7 @@ def stream_arm(args, world, rank):
             reqs.append((a, g, "pvc", opt - int(rng.integers(0, 2)), opt))
     max_n = max(g.n for g, _ in pool)
     lat, bad, budget, done = [], 0, 0, 0
+    lane_lat = {}
     with vcgpu.Server(max_vertices=max_n, max_requests=4096, mem_budget=2 << 30) as srv:
         lanes = srv.shape()
         for g, opt in pool[:32]:  # warm-up: kernel launch, first-touch of buffers
@@ -397,6 +399,7 @@ def stream_arm(args, world, rank):
                 g, kind, k, opt = outstanding.pop(tk)
                 done += 1
                 lat.append(r.total_ms)
+                lane_lat.setdefault(vcgpu.Server.lane(tk), []).append(r.total_ms)
                 if r.status == vcgpu.VC_BUDGET:
                     budget += 1
                 elif r.status != vcgpu.VC_OK:
@@ -409,6 +412,10 @@ def stream_arm(args, world, rank):
             time.sleep(max(0.0, min(nxt, 0.0005)))
         wall = time.perf_counter() - t0
     lat = np.asarray(lat)
+    for li, x in sorted(lane_lat.items()):
+        if li < len(lanes):
+            lanes[li].update({"requests": len(x), "p50_latency_ms": float(np.percentile(x, 50)),
+                              "p99_latency_ms": float(np.percentile(x, 99))})
     line = {"metric": METRIC, "value": done / wall, "unit": "requests/s", "n_gpus": 1, "steps": 1, "warmup": 1,
             "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic",

@@ -143,7 +143,7 @@ vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out);
  * (at most max_tickets, oldest first): lets a caller with many requests in
  * flight poll only the finished ones. No counterpart in the reference. */
 vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32_t max_tickets, uint32_t *count);
-/* The server's lanes (1 or 2) into shape[6*i..]: largest request (vertices),
+/* The server's lanes (1 to 3) into shape[6*i..]: largest request (vertices),
  * grid, block, search units, dynamic shared memory per CTA, dense (1) or CSR
  * (0) kernel; *lanes receives the lane count.  A diagnostic without a
  * counterpart in the reference. */

@@ -1,5 +1,7 @@
 // vc_dense.cuh -- the search for graphs of at most 255 vertices (the batched
-// workload's G(n, p) instances, n in [30, 200], and the 60-vertex case).
+// workload's G(n, p) instances, n in [30, 200], and the 60-vertex case), and,
+// with 20-word rows, for graphs of up to 640 vertices whose degrees all fit a
+// byte (at most 254).
 //
 // Same search as vc_search.cuh (the reference's degree-one, triangle and
 // high-degree rules, the E > b^2 prune and max-degree branching), with dense
@@ -33,8 +35,9 @@ namespace vcg {
 
 template <int NW>
 struct Rows {
-    static constexpr int kStride = NW >= 8 ? NW + 4 : NW;  // dense_row_words
-    static constexpr int kJ = NW >= 8 ? 2 : 1;              // degree words per lane
+    static constexpr int kStride = NW == 8 ? 12 : NW;  // dense_row_words
+    static constexpr int kJ = NW >= 8 ? NW / 4 : 1;     // degree words per lane
+    static constexpr int kCandBits = 4 * kJ >= 16 ? 5 : (4 * kJ >= 8 ? 4 : 3);  // bits of a lane's candidate count
     static constexpr int kTri = 32 * NW * kStride;          // offset of the triangle bitmap
 };
 
@@ -303,7 +306,7 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t pre = 0, total = 0;
 #pragma unroll
-    for (int b = 0; b < (J == 2 ? 4 : 3); ++b) {
+    for (int b = 0; b < Rows<NW>::kCandBits; ++b) {
         const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
         pre += __popc(bal & lt) << b;
         total += __popc(bal) << b;
@@ -501,7 +504,7 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
     const unsigned lane = lane_id();
     const InstDesc d = load_desc(&P.inst[inst]);
     const uint32_t *rp = P.row_ptr + d.row_off, *cl = P.col + d.col_off;
-    for (uint32_t i = lane; i < Rows<NW>::kTri + 8u; i += 32) adj[i] = 0;
+    for (uint32_t i = lane; i < Rows<NW>::kTri + (uint32_t)NW; i += 32) adj[i] = 0;
     __syncwarp();
     for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
         uint32_t *row = adj + v * Rows<NW>::kStride;

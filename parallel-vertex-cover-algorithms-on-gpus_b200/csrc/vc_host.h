@@ -72,15 +72,32 @@ struct Job {
     float kernel_ms = 0;
     unsigned long long t0 = 0;
     bool aborted = false;
+    bool wide = false;  // every graph may take the 20-word dense kernel
     Plan plan;
 };
 
+// The largest graph of the wide dense kernel; it also needs every degree <= 254.
+constexpr uint32_t kWideMaxN = 640;
+
+// True if a graph of n vertices (host row offsets) fits the wide dense kernel.
+inline bool wide_ok(uint32_t n, const uint32_t *row_ptr)
+{
+    if (n > kWideMaxN || !row_ptr) return false;
+    for (uint32_t v = 0; v < n; ++v)
+        if (row_ptr[v + 1] - row_ptr[v] > 254u) return false;
+    return true;
+}
+
+struct PlanOpts {
+    uint32_t smem_budget = 0;  // bytes per CTA for CSR workspaces, 0 = the device limit
+    uint32_t warp_max_np = 0;  // largest capacity given warp units, 0 = kWarpMaxNP
+    uint32_t warps = 0;        // warps per CTA with warp_gws, 0 = 8
+    bool wide = false;         // graphs of 256..640 vertices may take the wide dense kernel
+    bool warp_gws = false;     // warp units with global-memory workspaces
+};
+
 Ctx *get_ctx(int dev, vc_status *err);
-// smem_budget (bytes per CTA, 0 = the device limit) caps the CSR search units'
-// shared-memory workspaces; warp_max_np (0 = kWarpMaxNP) is the largest vertex
-// capacity given warp search units rather than 512-thread CTA units.
-cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, uint32_t smem_budget = 0,
-                      uint32_t warp_max_np = 0);
+cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOpts &o = PlanOpts());
 void cap_plan(const Ctx &c, Plan &pl, uint32_t per_sm);
 vc_status run_job(Ctx &c, Job &job, cudaStream_t stream);
 vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out);

@@ -88,6 +88,9 @@ struct SrvLane {
     uint64_t arena_bump = 0;
     uint64_t sub_tail = 0;
     bool running = false;
+    bool resident = false;  // launched at creation and kept running (no idle exit)
+    bool draining = false;  // a resident kernel asked to stop before its time limit
+    std::chrono::steady_clock::time_point t_launch;
     bool stop = false;
     bool discard_queue = false;
     vc_status fatal = VC_OK;
@@ -141,13 +144,36 @@ vc_status launch_kernel(SrvLane *s)
     P.subq = (const uint32_t *)s->subq.p;
     P.hres = s->d_res;
     P.hres_words = s->res_words;
-    P.idle_ns = 200ull * 1000000ull;
+    P.idle_ns = s->resident ? (1ull << 62) : 200ull * 1000000ull;
     void *args[] = {&P};
+    // the batched path may have lowered the kernel's shared-memory limit; and
+    // SMs hosting this lane keep their largest shared-memory configuration, so
+    // the other lanes' CTAs can be placed beside it
+    if (cudaFuncSetAttribute(s->pl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->pl.smem) != cudaSuccess ||
+        cudaFuncSetAttribute(s->pl.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+        return VC_ERR_CUDA;
     if (cudaLaunchCooperativeKernel(s->pl.fn, dim3(s->pl.grid), dim3(s->pl.block), args, s->pl.smem, s->kstream) !=
         cudaSuccess)
         return VC_ERR_CUDA;
     s->running = true;
+    s->t_launch = std::chrono::steady_clock::now();
     return VC_OK;
+}
+
+// Waits (bounded) until every CTA of the lane's launch has started: the next
+// lane's kernel is then placed in what this one leaves free on each SM.
+bool wait_resident(SrvLane *s)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    while (std::chrono::steady_clock::now() - t0 < std::chrono::seconds(5)) {
+        unsigned long long n = 0;
+        if (cudaMemcpy(&n, (unsigned long long *)s->ctl.p + kStarted, sizeof(n), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return false;
+        if (n >= s->pl.grid) return true;
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    return false;
 }
 
 // Admits pending requests into free slots (called by the loop, lock held):
@@ -304,6 +330,7 @@ void request_loop(SrvLane *s)
         bool progress = false;
         if (s->running && cudaStreamQuery(s->kstream) != cudaErrorNotReady) {
             s->running = false;
+            s->draining = false;
             // the kernel exited: everything it claimed has finished unless it stopped at its limit
             collect(s);
             unsigned long long abort_flag = 0;
@@ -317,15 +344,25 @@ void request_loop(SrvLane *s)
             // through the non-coherent cache).  When it is full, in-flight work
             // drains, the kernel is asked to stop, and the arena restarts empty.
             if (!s->running && s->inflight.empty()) s->arena_bump = 0;
+            // a resident kernel is restarted well before its 600 s limit: it
+            // drains (no admissions) and exits, and the loop relaunches it
+            if (s->resident && s->running && !s->draining &&
+                std::chrono::steady_clock::now() - s->t_launch > std::chrono::seconds(480)) {
+                s->draining = true;
+                unsigned long long one = 1;
+                cudaMemcpyAsync((unsigned long long *)s->ctl.p + kShutdown, &one, sizeof(one), cudaMemcpyHostToDevice,
+                                s->cstream);
+                cudaStreamSynchronize(s->cstream);
+            }
             bool arena_full = false;
-            if (admit(s, lk, arena_full)) progress = true;
+            if (!s->draining && admit(s, lk, arena_full)) progress = true;
             if (arena_full && s->inflight.empty() && s->running) {
                 unsigned long long one = 1;
                 cudaMemcpyAsync((unsigned long long *)s->ctl.p + kShutdown, &one, sizeof(one), cudaMemcpyHostToDevice,
                                 s->cstream);
                 cudaStreamSynchronize(s->cstream);
             }
-            if (!s->inflight.empty() && !s->running) {
+            if ((!s->inflight.empty() || s->resident) && !s->running) {
                 vc_status st = launch_kernel(s);
                 if (st != VC_OK) s->fatal = st;
                 progress = true;
@@ -354,14 +391,19 @@ void request_loop(SrvLane *s)
     s->cv.notify_all();
 }
 
+// Asks a lane's loop to stop; its kernel drains and exits.
+void lane_stop(SrvLane *s)
+{
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv.notify_all();
+}
+
 void lane_destroy(SrvLane *s)
 {
     if (!s) return;
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->stop = true;
-        s->cv.notify_all();
-    }
+    lane_stop(s);
     if (s->loop.joinable()) s->loop.join();
     s->desc.release();
     s->st.release();
@@ -379,9 +421,11 @@ void lane_destroy(SrvLane *s)
 }
 
 // A lane for requests of at most max_n vertices with the given plan.
-vc_status lane_create(Ctx *c, uint64_t budget, uint32_t slots, uint32_t max_n, const Plan &pl, SrvLane **out)
+vc_status lane_create(Ctx *c, uint64_t budget, uint32_t slots, uint32_t max_n, const Plan &pl, bool resident,
+                      SrvLane **out)
 {
     SrvLane *s = new SrvLane();
+    s->resident = resident;
     s->dev = c->dev;
     s->ctx = c;
     s->slots = slots;
@@ -411,65 +455,134 @@ vc_status lane_create(Ctx *c, uint64_t budget, uint32_t slots, uint32_t max_n, c
     memset(s->h_res, 0, res_bytes);
     s->info.resize(s->slots);
     for (uint32_t i = 0; i < s->slots; ++i) s->free_slots.push_back(s->slots - 1 - i);
+    if (resident) {  // launched now, in the order the lanes are created
+        vc_status e = launch_kernel(s);
+        if (e != VC_OK) {
+            lane_destroy(s);
+            return e;
+        }
+        // Bounded wait for all CTAs to start, so that the next lane is placed
+        // around them.  If it runs out the lane still serves; only its
+        // placement is left to the block scheduler.
+        wait_resident(s);
+    }
     s->loop = std::thread(request_loop, s);
     *out = s;
     return VC_OK;
 }
 
-constexpr uint32_t kDenseMax = 255;       // the dense lane's largest request
-constexpr uint32_t kDenseCtasPerSm = 3;   // its CTAs per SM when it shares the device
+constexpr uint32_t kDenseMax = 255;  // the narrow dense lane's largest request
 
-// Plans the two lanes so that kDenseCtasPerSm dense CTAs and one CSR CTA fit
-// on every SM together (registers, shared memory, warps, CTAs).  Returns false
-// when the CSR lane cannot fit beside the dense one.
-bool plan_split(Ctx &c, uint32_t max_n, Plan &pd, Plan &ps)
+// A lane's kernel shape and how many of its CTAs it places on each SM.
+struct LaneSpec {
+    Plan pl;
+    uint32_t max_n = 0;
+    uint32_t per_sm = 0;
+    bool resident = false;
+};
+
+struct SmRes {
+    int regs = 0, smem = 0, reserved = 0, warps = 0, blocks = 0;
+};
+
+// Registers, shared memory, warps and CTAs that `per_sm` CTAs of a plan take on one SM.
+bool sm_use(const Plan &pl, uint32_t per_sm, const SmRes &r, uint64_t use[4])
 {
-    if (make_plan(c, 32 * 8, kDenseMax, pd) != cudaSuccess || !pd.dense) return false;
-    int regs_sm = 0, smem_sm = 0, reserved = 0, warps_sm = 0, blocks_sm = 0;
-    if (cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c.dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, c.dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&warps_sm, cudaDevAttrMaxThreadsPerMultiProcessor, c.dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, c.dev) != cudaSuccess)
-        return false;
-    warps_sm /= 32;
-    cudaFuncAttributes fd;
-    if (cudaFuncGetAttributes(&fd, pd.fn) != cudaSuccess) return false;
-    auto warp_regs = [](int regs) { return (uint32_t)((regs * 32 + 255) / 256 * 256); };  // per-warp allocation
-    const uint32_t d_regs = kDenseCtasPerSm * (pd.block / 32) * warp_regs(fd.numRegs);
-    const uint32_t d_smem = kDenseCtasPerSm * (pd.smem + (uint32_t)fd.sharedSizeBytes + (uint32_t)reserved);
-    if (d_regs >= (uint32_t)regs_sm || d_smem + (uint32_t)reserved >= (uint32_t)smem_sm) return false;
-    const uint32_t smem_left = (uint32_t)smem_sm - d_smem - (uint32_t)reserved;
-    const uint32_t np = std::max<uint32_t>(32, (max_n + 31) / 32 * 32);
-    // warp units for the CSR lane at any size whose workspace fits beside the
-    // dense CTAs: more units than one 512-thread CTA per SM
-    if (make_plan(c, np, max_n, ps, smem_left, 1u << 16) != cudaSuccess || ps.dense) return false;
-    cudaFuncAttributes fs;
-    if (cudaFuncGetAttributes(&fs, ps.fn) != cudaSuccess) return false;
-    const bool fits = d_regs + (ps.block / 32) * warp_regs(fs.numRegs) <= (uint32_t)regs_sm &&
-                      d_smem + ps.smem + (uint32_t)fs.sharedSizeBytes + (uint32_t)reserved <= (uint32_t)smem_sm &&
-                      kDenseCtasPerSm * (pd.block / 32) + ps.block / 32 <= (uint32_t)warps_sm &&
-                      kDenseCtasPerSm + 1 <= (uint32_t)blocks_sm;
-    if (!fits) return false;
-    cap_plan(c, pd, kDenseCtasPerSm);
-    cap_plan(c, ps, 1);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, pl.fn) != cudaSuccess) return false;
+    const uint64_t warp_regs = (uint64_t)(fa.numRegs * 32 + 255) / 256 * 256;  // per-warp allocation unit
+    use[0] += per_sm * (pl.block / 32) * warp_regs;
+    use[1] += per_sm * ((uint64_t)pl.smem + fa.sharedSizeBytes + (uint64_t)r.reserved);
+    use[2] += per_sm * (pl.block / 32);
+    use[3] += per_sm;
     return true;
+}
+
+bool fits(const uint64_t use[4], const SmRes &r)
+{
+    return use[0] <= (uint64_t)r.regs && use[1] <= (uint64_t)r.smem && use[2] <= (uint64_t)r.warps &&
+           use[3] <= (uint64_t)r.blocks;
+}
+
+// Lanes for requests of up to max_n (> 255) vertices: the narrow dense lane
+// (n <= 255), the wide dense lane (256..640 vertices, byte degrees) and a CSR
+// lane for the rest, returned in that order.  Their CTAs share every SM, and
+// each placement is forced by what is free on the SMs rather than left to the
+// block scheduler: the wide lane's CTAs are padded to more than half an SM's
+// shared memory (so one per SM) and launched first; the narrow lane, launched
+// next, finds room for exactly three CTAs per SM; the CSR lane (launched on
+// demand) finds registers for exactly one.  Any lane relaunched later fits the
+// same way into what the others leave.  The two dense lanes stay resident.
+// Returns an empty list when this does not fit the device.
+std::vector<LaneSpec> plan_lanes(Ctx &c, uint32_t max_n)
+{
+    std::vector<LaneSpec> none;
+    SmRes r;
+    if (cudaDeviceGetAttribute(&r.regs, cudaDevAttrMaxRegistersPerMultiprocessor, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&r.smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&r.reserved, cudaDevAttrReservedSharedMemoryPerBlock, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&r.warps, cudaDevAttrMaxThreadsPerMultiProcessor, c.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&r.blocks, cudaDevAttrMaxBlocksPerMultiprocessor, c.dev) != cudaSuccess)
+        return none;
+    r.warps /= 32;
+    LaneSpec narrow, wide, csr;
+    narrow.max_n = kDenseMax;
+    narrow.per_sm = 3;
+    narrow.resident = true;
+    if (make_plan(c, 32 * 8, kDenseMax, narrow.pl) != cudaSuccess || !narrow.pl.dense) return none;
+    wide.max_n = std::min(max_n, kWideMaxN);
+    wide.per_sm = 1;
+    wide.resident = true;
+    PlanOpts wo;
+    wo.wide = true;
+    if (make_plan(c, 32 * 20, kWideMaxN, wide.pl, wo) != cudaSuccess || !wide.pl.dense) return none;
+    cudaFuncAttributes fw;
+    if (cudaFuncGetAttributes(&fw, wide.pl.fn) != cudaSuccess) return none;
+    // padding: two of the wide CTAs must not fit on one SM
+    const uint32_t half = (uint32_t)r.smem / 2 + 1 - (uint32_t)fw.sharedSizeBytes - (uint32_t)r.reserved;
+    wide.pl.smem = std::max(wide.pl.smem, half);
+    if (wide.pl.smem > (uint32_t)c.smem_optin) return none;
+    const uint32_t np = std::max<uint32_t>(32, (max_n + 31) / 32 * 32);
+    uint64_t use[4] = {0, 0, 0, 0};
+    if (!sm_use(wide.pl, 1, r, use) || !sm_use(narrow.pl, narrow.per_sm, r, use) || !fits(use, r)) return none;
+    {   // exactly three narrow CTAs beside the wide one: a fourth must not fit
+        uint64_t u4[4] = {use[0], use[1], use[2], use[3]};
+        if (sm_use(narrow.pl, 1, r, u4) && fits(u4, r)) return none;
+    }
+    for (uint32_t warps = 8; warps >= 1; warps >>= 1) {
+        csr.max_n = max_n;
+        csr.per_sm = 1;
+        PlanOpts so;
+        so.warp_gws = true;
+        so.warp_max_np = 1u << 16;
+        so.warps = warps;
+        if (make_plan(c, np, max_n, csr.pl, so) != cudaSuccess || csr.pl.dense) continue;
+        uint64_t u3[4] = {use[0], use[1], use[2], use[3]};
+        if (!sm_use(csr.pl, 1, r, u3) || !fits(u3, r)) continue;
+        uint64_t u5[4] = {u3[0], u3[1], u3[2], u3[3]};  // and a second CSR CTA must not fit
+        if (sm_use(csr.pl, 1, r, u5) && fits(u5, r)) continue;
+        std::vector<LaneSpec> lanes{narrow, wide, csr};
+        for (LaneSpec &l : lanes) cap_plan(c, l.pl, l.per_sm);
+        return lanes;
+    }
+    return none;
 }
 
 }  // namespace
 
-// Public handle: the lanes; a ticket carries its lane in the low bit.
+// Public handle: the lanes; a ticket carries its lane in its low two bits.
 struct vc_server {
     std::vector<SrvLane *> lanes;
     uint32_t max_n = 0;
+    bool wide_lane = false;  // lanes[1] is the wide dense lane
 };
 
 namespace {
 inline SrvLane *lane_of(vc_server *s, uint64_t ticket, uint64_t *lt)
 {
-    const uint32_t li = (uint32_t)(ticket & 1u);
+    const uint32_t li = (uint32_t)(ticket & 3u);
     if (li >= s->lanes.size()) return nullptr;
-    *lt = ticket >> 1;
+    *lt = ticket >> 2;
     return s->lanes[li];
 }
 }  // namespace
@@ -490,17 +603,24 @@ extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes,
     if (max_n > kMaxVertices) return VC_ERR_TOO_LARGE;
     vc_server *s = new vc_server();
     s->max_n = max_n;
-    Plan pd, ps;
-    if (max_n > kDenseMax && !c->force_sparse && plan_split(*c, max_n, pd, ps)) {
-        SrvLane *a = nullptr, *b = nullptr;
-        vc_status e = lane_create(c, budget / 2, slots, kDenseMax, pd, &a);
-        if (e == VC_OK) e = lane_create(c, budget - budget / 2, slots, max_n, ps, &b);
-        if (e != VC_OK) {
-            lane_destroy(a);
-            delete s;
-            return e;
+    std::vector<LaneSpec> specs;
+    if (max_n > kDenseMax && !c->force_sparse) specs = plan_lanes(*c, max_n);
+    if (!specs.empty()) {
+        // device memory for admitted graphs: half to the narrow dense lane;
+        // the wide lane is created (and launched) first, see plan_lanes
+        const uint64_t share[3] = {budget / 2, budget / 4, budget - budget / 2 - budget / 4};
+        SrvLane *made[3] = {nullptr, nullptr, nullptr};
+        for (int i : {1, 0, 2}) {
+            vc_status e = lane_create(c, share[i], slots, specs[i].max_n, specs[i].pl, specs[i].resident, &made[i]);
+            if (e != VC_OK) {
+                for (SrvLane *x : made) lane_stop(x);
+                for (SrvLane *x : made) lane_destroy(x);
+                delete s;
+                return e;
+            }
         }
-        s->lanes = {a, b};
+        s->lanes = {made[0], made[1], made[2]};
+        s->wide_lane = true;
     } else {
         Plan pl;
         if (make_plan(*c, std::max<uint32_t>(32, (max_n + 31) / 32 * 32), max_n, pl) != cudaSuccess) {
@@ -508,7 +628,7 @@ extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes,
             return VC_ERR_CUDA;
         }
         SrvLane *a = nullptr;
-        vc_status e = lane_create(c, budget, slots, max_n, pl, &a);
+        vc_status e = lane_create(c, budget, slots, max_n, pl, false, &a);
         if (e != VC_OK) {
             delete s;
             return e;
@@ -530,7 +650,10 @@ extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_re
         vc_status v = validate_csr(g);
         if (v != VC_OK) return v;
     }
-    const uint32_t li = (s->lanes.size() > 1 && g->n <= kDenseMax) ? 0u : (uint32_t)s->lanes.size() - 1u;
+    // lane: narrow dense, wide dense (byte degrees, up to 640 vertices), else CSR
+    uint32_t li = (uint32_t)s->lanes.size() - 1u;
+    if (s->lanes.size() > 1 && g->n <= kDenseMax) li = 0;
+    else if (s->wide_lane && wide_ok(g->n, g->row_ptr)) li = 1;
     SrvLane *l = s->lanes[li];
     Pending p;
     p.n = g->n;
@@ -543,7 +666,7 @@ extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_re
     if (l->stop) return VC_ERR_INVALID;
     if (l->fatal != VC_OK) return l->fatal;
     p.ticket = l->next_ticket++;
-    *ticket = (p.ticket << 1) | li;
+    *ticket = (p.ticket << 2) | li;
     l->pending.push_back(std::move(p));
     l->cv.notify_all();
     return VC_OK;
@@ -588,7 +711,7 @@ extern "C" vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32
         while (k < max_tickets && !l->ready.empty()) {
             const uint64_t t = l->ready.front();
             l->ready.pop_front();
-            if (l->done.count(t)) tickets[k++] = (t << 1) | li;  // skip tickets already collected by vc_server_poll
+            if (l->done.count(t)) tickets[k++] = (t << 2) | li;  // skip tickets already collected by vc_server_poll
         }
     }
     *count = k;
@@ -601,7 +724,7 @@ extern "C" vc_status vc_server_shape(vc_server *s, uint32_t *shape, uint32_t max
     *lanes = (uint32_t)s->lanes.size();
     for (uint32_t i = 0; i < s->lanes.size() && i < max_lanes; ++i) {
         const SrvLane *l = s->lanes[i];
-        uint32_t *o = shape + 6 * i;
+        uint32_t *o = shape + 6 * i;  // per lane
         o[0] = l->max_n;
         o[1] = l->pl.grid;
         o[2] = l->pl.block;
@@ -615,6 +738,9 @@ extern "C" vc_status vc_server_shape(vc_server *s, uint32_t *shape, uint32_t max
 extern "C" vc_status vc_server_destroy(vc_server *s)
 {
     if (!s) return VC_ERR_INVALID;
+    // all lanes stop together: a lane's kernel can only finish once all its
+    // CTAs have run, which may need another lane's kernel to leave its SMs
+    for (SrvLane *l : s->lanes) lane_stop(l);
     for (SrvLane *l : s->lanes) lane_destroy(l);
     delete s;
     return VC_OK;

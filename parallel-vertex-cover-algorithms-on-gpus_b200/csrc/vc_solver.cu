@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Param
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint32_t cp_hdr[kCpHdrWords];
+    if (P.server && threadIdx.x == 0) atomicAdd(&P.ctl[kStarted], 1ull);  // residency check of server lanes
     const uint32_t su_per_cta = NT / G::kSize;
     CtaPool cp;
     cp.su = su_per_cta;
@@ -66,7 +67,9 @@ __global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Param
 #endif
 template <int NW>
 struct DenseOcc {
-    static constexpr unsigned kThreads = NW >= 8 ? VC_DENSE8_THREADS : VC_DENSE4_THREADS;
+    // 20-word graphs: three 256-thread CTAs' worth of registers (80 per thread),
+    // so that a server lane of them fits beside three 8-word CTAs per SM
+    static constexpr unsigned kThreads = NW >= 16 ? 768u : (NW >= 8 ? VC_DENSE8_THREADS : VC_DENSE4_THREADS);
     template <unsigned NT>
     static constexpr unsigned min_ctas() { return kThreads / NT < 32 ? kThreads / NT : 32; }  // 32 CTAs/SM at most
 };
@@ -76,6 +79,7 @@ __global__ void __launch_bounds__(NT, DenseOcc<NW>::template min_ctas<NT>()) k_d
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint32_t cp_hdr[kCpHdrWords];
+    if (P.server && threadIdx.x == 0) atomicAdd(&P.ctl[kStarted], 1ull);  // residency check of server lanes
     const uint32_t su_per_cta = NT / 32;
     uint32_t *adj = reinterpret_cast<uint32_t *>(smem);
     uint8_t *ws0 = smem + dense_adj_bytes(NW);
@@ -254,19 +258,40 @@ static cudaError_t plan_dense(Ctx &c, Plan &pl)
     return cudaSuccess;
 }
 
-cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, uint32_t smem_budget, uint32_t warp_max_np)
+cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOpts &o)
 {
     pl.dense = false;
-    // dense bitsets up to 255 vertices (degrees are bytes, 0xFF marks a removed vertex)
+    const uint32_t smem_budget = o.smem_budget, warp_max_np = o.warp_max_np;
+    // dense bitsets up to 255 vertices, and up to 640 when every degree fits a
+    // byte (degrees are bytes; 0 = removed or isolated)
     if (nmax <= 64 && !c.force_sparse) return plan_dense<2>(c, pl);
     if (nmax <= 128 && !c.force_sparse) return plan_dense<4>(c, pl);
     if (nmax <= 255 && !c.force_sparse) return plan_dense<8>(c, pl);
+    if (nmax <= kWideMaxN && o.wide && !c.force_sparse) return plan_dense<20>(c, pl);
     pl.np = np;
     pl.su_bytes = su_workspace_bytes(np);
     pl.stride = (4 + np / 32 + 3) / 4 * 4;
     const uint32_t static_smem = 1024;  // reductions / broadcasts / CTA pool header
     uint32_t budget = (uint32_t)c.smem_optin - static_smem;
     if (smem_budget) budget = std::min(budget, smem_budget > static_smem ? smem_budget - static_smem : 0u);
+    if (np <= (warp_max_np ? warp_max_np : kWarpMaxNP) && o.warp_gws) {
+        // warp units with their workspaces in global memory: the CTA holds
+        // only its pool
+        uint32_t warps = o.warps ? o.warps : 8;
+        pl.cta_slots = warps > 1 ? 2 * warps : 0;
+        const uint32_t smem = cta_pool_bytes(pl.cta_slots, pl.stride);
+        cudaError_t e;
+        switch (warps) {
+        case 8: e = plan_variant<WarpG, 256>(c, pl, smem); break;
+        case 4: e = plan_variant<WarpG, 128>(c, pl, smem); break;
+        case 2: e = plan_variant<WarpG, 64>(c, pl, smem); break;
+        default: e = plan_variant<WarpG, 32>(c, pl, smem); break;
+        }
+        if (e != cudaSuccess) return e;
+        pl.num_su = pl.grid * (pl.block / 32);
+        pl.global_ws = true;
+        return cudaSuccess;
+    }
     if (np <= (warp_max_np ? warp_max_np : kWarpMaxNP)) {
         uint32_t warps = 8;
         while (warps > 1 && warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget) warps >>= 1;
@@ -324,7 +349,9 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     }
     uint32_t np = std::max<uint32_t>(32, (nmax + 31) / 32 * 32);
     Plan pl;
-    if (make_plan(c, np, nmax, pl) != cudaSuccess) return VC_ERR_CUDA;
+    PlanOpts po;
+    po.wide = job.wide;
+    if (make_plan(c, np, nmax, pl, po) != cudaSuccess) return VC_ERR_CUDA;
     const uint32_t stride = pl.stride;
     uint32_t q = 1024;
     while (q < 2 * pl.num_su) q <<= 1;
@@ -559,6 +586,7 @@ extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result 
     d.pad = 0;
     job.desc.push_back(d);
     job.time_limit_s = req->time_limit_s;
+    job.wide = !dev_in && wide_ok(g->n, g->row_ptr);
     vc_status s = run_job(*c, job, stream);
     if (s != VC_OK) { out->status = s; return s; }
     s = fill_result(job, 0, req->instance == VC_MVC ? req->ub : 0, out);
@@ -635,22 +663,29 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         job.d_rp = (const uint32_t *)c->rp.p;
         job.d_col = (const uint32_t *)c->col.p;
     }
-    // One launch per kernel shape: dense bitsets (n <= 255), warp search units
-    // (n <= kWarpMaxNP), CTA search units (larger); the shape is sized by the
-    // largest graph of its class, so small graphs never run in a large graph's
-    // workspace.
-    auto klass = [](uint32_t n) { return n <= 255 ? 0 : (n <= kWarpMaxNP ? 1 : 2); };
+    // One launch per kernel shape: dense bitsets (n <= 255), wide dense bitsets
+    // (n <= 640, every degree <= 254), warp search units (n <= kWarpMaxNP), CTA
+    // search units (larger); the shape is sized by the largest graph of its
+    // class, so small graphs never run in a large graph's workspace.  The row
+    // offsets are host arrays on both entry points.
+    auto klass = [&](uint32_t i) {
+        const uint32_t n = a->n[i];
+        if (n <= 255) return 0;
+        if (wide_ok(n, a->row_ptr + a->row_off[i])) return 1;
+        return n <= kWarpMaxNP ? 2 : 3;
+    };
     vc_status first = VC_OK;
     float total_kernel = 0;
     std::vector<uint32_t> members;
-    for (int cl = 0; cl < 3; ++cl) {
+    for (int cl = 0; cl < 4; ++cl) {
         members.clear();
         for (uint32_t i = 0; i < count; ++i)
-            if (a->n[i] > 0 && klass(a->n[i]) == cl) members.push_back(i);
+            if (a->n[i] > 0 && klass(i) == cl) members.push_back(i);
         if (members.empty()) continue;
         Job cj;
         cj.d_rp = job.d_rp;
         cj.d_col = job.d_col;
+        cj.wide = cl == 1;
         cj.desc.resize(members.size());
         double tl = 0;
         for (size_t j = 0; j < members.size(); ++j) {

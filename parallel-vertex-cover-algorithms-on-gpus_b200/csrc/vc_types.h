@@ -28,7 +28,8 @@ enum : uint32_t {
     kSubTail = 112,   // server: submissions published by the host
     kShutdown = 128,  // server: the host asks the kernel to exit once idle
     kLastWork = 144,  // server: %globaltimer of the last claimed submission
-    kCtlWords = 160
+    kStarted = 160,   // server: CTAs of the launch that have started
+    kCtlWords = 176
 };
 
 enum : uint32_t { kModeMVC = 0, kModePVC = 1 };
@@ -111,15 +112,17 @@ VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
     return (b + 15u) & ~15u;
 }
 
-// Dense-bitset search unit (graphs of at most 255 vertices, nw <= 8 words):
-// per CTA adj[32*nw][dense_row_words(nw)] u32, then tri[8] u32 (the vertices
+// Dense-bitset search unit (nw = 2, 4 or 8 words: graphs of at most 255
+// vertices; nw = 20: up to 640 vertices whose degrees are all at most 254):
+// per CTA adj[32*nw][dense_row_words(nw)] u32, then tri[nw] u32 (the vertices
 // that lie on a triangle of the staged graph); per warp
 //   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 |
 //   cand[32*nw] u16 | degs[32*nw] u8
 // Row stride in words: 8-word rows are padded to 12 so that the 16-byte row
-// loads of eight consecutive lanes fall in distinct shared-memory banks.
-VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw >= 8 ? nw + 4 : nw; }
-VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw) + 32u; }
+// loads of eight consecutive lanes fall in distinct shared-memory banks
+// (20-word rows already do).
+VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw == 8 ? 12u : nw; }
+VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw) + 128u; }
 VC_HD inline uint32_t dense_workspace_bytes(uint32_t nw)
 {
     uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 2u * 32u * nw + 32u * nw;

@@ -287,12 +287,17 @@ class Server:
     def shape(self) -> List[dict]:
         """The server's lanes: largest request, grid, block, search units, shared
         memory per CTA and kernel kind."""
-        buf = np.zeros(12, dtype=np.uint32)
+        buf = np.zeros(18, dtype=np.uint32)
         cnt = ctypes.c_uint32(0)
-        lib().vc_server_shape(self._h, buf.ctypes.data, 2, ctypes.byref(cnt))
+        lib().vc_server_shape(self._h, buf.ctypes.data, 3, ctypes.byref(cnt))
         return [{"max_vertices": int(buf[6 * i]), "grid": int(buf[6 * i + 1]), "block": int(buf[6 * i + 2]),
                  "search_units": int(buf[6 * i + 3]), "smem_bytes": int(buf[6 * i + 4]),
-                 "kernel": "dense" if buf[6 * i + 5] else "csr"} for i in range(min(int(cnt.value), 2))]
+                 "kernel": "dense" if buf[6 * i + 5] else "csr"} for i in range(min(int(cnt.value), 3))]
+
+    @staticmethod
+    def lane(ticket: int) -> int:
+        """The lane a ticket's request runs in (its low two bits)."""
+        return int(ticket) & 3
 
     def wait(self, ticket: int, timeout: float = 120.0, want_cover: bool = True) -> Solution:
         import time

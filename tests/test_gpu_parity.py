@@ -231,3 +231,58 @@ def test_time_limit_returns_timeout_and_device_stays_usable():
     g1 = W.config1_graph()
     small = json.load(open(os.path.join(GOLDEN, "small.json")))
     _check_mvc(g1, vcgpu.solve(g1, "mvc", time_limit=TL), small["config1"]["opt"])
+
+
+def _wide_graphs():
+    """Graphs of 256..640 vertices with small degrees (the wide dense kernel's
+    range) with their optima: G(n, p) at average degree 3.2 solved by the
+    oracle, and the served stream's pinned pool graphs of that size."""
+    rng = np.random.default_rng(4242)
+    out = []
+    for n in (260, 330, 400, 480, 560, 640):
+        g = W.gnp(n, 3.2 / (n - 1), int(rng.integers(1 << 30)))
+        st, opt, _, _ = O.mvc(g, node_limit=300_000)
+        if st == O.OK:
+            out.append((g, opt))
+    recs = [json.loads(l) for l in open(os.path.join(GOLDEN, "stream_seed0.jsonl")) if l.strip()]
+    for r in sorted(recs, key=lambda r: r["i"]):
+        if r["status"] == "ok" and 255 < r["n"] <= 640 and r["nodes"] <= 300_000:
+            out.append((W.stream_instance(r["i"]), r["opt"]))
+    return out
+
+
+def test_wide_dense_kernel_batched_and_plain():
+    """256..640 vertices with byte degrees run on the 20-word dense kernel,
+    batched and one at a time, with the oracle's optima and decisions."""
+    items = _wide_graphs()
+    assert len(items) >= 8
+    graphs = [g for g, _ in items]
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    assert st == vcgpu.VC_OK
+    _, shape = vcgpu.debug_stats()
+    assert int(shape[4]) >> 31 == 1 and (int(shape[4]) & 0x7FFFFFFF) == 640, shape  # the wide dense plan ran
+    for (g, opt), r in zip(items, sols):
+        _check_mvc(g, r, opt)
+    for g, opt in items[::3]:
+        _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+        _check_pvc(g, vcgpu.solve(g, "pvc", k=opt - 1, time_limit=TL), opt - 1, 0)
+        _check_pvc(g, vcgpu.solve(g, "pvc", k=opt, time_limit=TL), opt, 1)
+
+
+def test_wide_range_with_a_high_degree_vertex_takes_csr():
+    """A 300-vertex graph with a vertex of degree 280 does not fit byte degrees:
+    it runs on the CSR kernel and stays exact."""
+    rng = np.random.default_rng(7)
+    n = 300
+    base = W.gnp(n, 2.5 / (n - 1), 99)
+    e = [(u, v) for u in range(n) for v in base.col[base.row_ptr[u]:base.row_ptr[u + 1]] if u < v]
+    hub = set(int(x) for x in rng.choice(np.arange(1, n), 280, replace=False))
+    e = list({(min(u, v), max(u, v)) for u, v in e + [(0, h) for h in hub]})
+    g = W.from_edges(n, np.asarray(e, dtype=np.int64), "hub300")
+    assert int(np.diff(g.row_ptr).max()) > 254
+    st, opt, _, _ = O.mvc(g, node_limit=2_000_000)
+    assert st == O.OK
+    r = vcgpu.solve(g, "mvc", time_limit=TL)
+    _, shape = vcgpu.debug_stats()
+    assert int(shape[4]) >> 31 == 0, shape  # CSR plan
+    _check_mvc(g, r, opt)

@@ -135,13 +135,14 @@ def test_server_completed_reports_each_ticket_once():
         assert srv.completed() == []
 
 
-def test_server_two_lanes_small_and_large():
+def test_server_lanes_small_and_large():
     """With max_vertices above 255 the server runs a dense lane for small
-    requests and a CSR lane for large ones side by side; results match the
-    oracle-pinned optima alone and in a mix, and both lanes take requests."""
+    requests, a wide dense lane for 256..640 vertices with byte degrees and a
+    CSR lane for the rest, side by side; results match the oracle-pinned optima
+    alone and in a mix, and each request runs in its lane."""
     recs = [json.loads(l) for l in open(os.path.join(GOLDEN, "stream_seed0.jsonl"))]
     pinned = sorted([r for r in recs if r["status"] == "ok" and r["nodes"] <= 300_000], key=lambda r: r["i"])
-    large = [r for r in pinned if r["n"] > 255][:6]
+    large = [r for r in pinned if r["n"] > 255][:6] + [r for r in pinned if r["n"] > 640][:2]
     small = [r for r in pinned if r["n"] <= 255][:18]
     assert large and small
     items = [(W.stream_instance(r["i"]), r["opt"]) for r in large + small]
@@ -152,7 +153,10 @@ def test_server_two_lanes_small_and_large():
         tickets = [srv.submit(g, "mvc") for g, _ in items]
         tickets += [srv.submit(g, "pvc", k=opt - 1) for g, opt in items[::3]]
         res = [srv.wait(t) for t in tickets]
-    assert {t & 1 for t in tickets} == {0, 1}
+    for t, (g, _) in zip(tickets, items):  # narrow dense, wide dense (byte degrees), CSR
+        deg_ok = int(np.diff(g.row_ptr).max()) <= 254
+        want = 0 if g.n <= 255 else (1 if g.n <= 640 and deg_ok else 2)
+        assert vcgpu.Server.lane(t) == want, (g.n, vcgpu.Server.lane(t))
     for (g, opt), r in zip(items, res):
         _check(g, r, "mvc", 0, opt)
     for (g, opt), r in zip(items[::3], res[len(items):]):
