@@ -123,17 +123,22 @@ vc_status vc_solve_batch(const vc_csr_arena *arena, const vc_request *reqs, vc_r
 vc_status vc_solve_batch_device(const vc_csr_arena *arena, const uint32_t *d_row_ptr, const uint32_t *d_col,
                                 const vc_request *reqs, vc_result *out);
 
-/* Continuous-batching server (no counterpart in the reference).  A persistent
- * kernel admits requests while others run; graphs and search state stay on the
- * device.  mem_budget_bytes bounds the device arena holding admitted graphs
- * (0 = 1 GiB); max_requests is the number of device slots (0 = 1024);
- * max_vertices is the largest graph accepted (0 = 1024; <= 255 selects the
- * dense-bitset kernel).  A request is admitted when a slot and arena room for
- * its CSR are free.  submit validates and copies the graph and returns a
- * ticket; poll returns VC_PENDING until the ticket's result is ready, then
- * fills *out (out->cover_mask, if non-NULL, receives n bytes; total_ms is the
- * time from submit to completion) and releases the ticket.  While a server
- * runs on a device, its persistent kernel holds that device's SMs. */
+/* Continuous-batching server (no counterpart in the reference).  Persistent
+ * kernels admit requests while others run; graphs and search state stay on the
+ * device.  mem_budget_bytes bounds the device arenas holding admitted graphs
+ * (0 = 1 GiB); max_requests is the number of device slots per lane (0 = 1024);
+ * max_vertices is the largest graph accepted (0 = 1024).  With max_vertices <=
+ * 255 there is one lane, the dense-bitset kernel on the whole device.  Above
+ * that there are three lanes side by side on every SM: requests of at most
+ * 255 vertices run in the dense lane, requests of 256..640 vertices whose
+ * degrees are all at most 254 in the wide dense lane, the rest in a CSR lane;
+ * the two dense lanes' kernels stay resident while the server lives.  A
+ * request is admitted when a slot and arena room for its CSR are free in its
+ * lane.  submit validates and copies the graph and returns a ticket (its lane
+ * in the low two bits); poll returns VC_PENDING until the ticket's result is
+ * ready, then fills *out (out->cover_mask, if non-NULL, receives n bytes;
+ * total_ms is the time from submit to completion) and releases the ticket.
+ * While a server runs on a device, its kernels hold that device's SMs. */
 typedef struct vc_server vc_server;
 vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests, uint32_t max_vertices,
                            vc_server **out);
