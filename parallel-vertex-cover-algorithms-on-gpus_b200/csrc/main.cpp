@@ -56,6 +56,7 @@ struct Config {
     unsigned startingDepth = 4;
     const char *outputFilePrefix = "1";
     const char *graphFileName = "GraphInput.txt";
+    bool zeroBased = false;  // -z: vertex ids in the file start at 0
 };
 
 void usage()
@@ -74,7 +75,8 @@ void usage()
             "   -d <Starting Depth>   recorded in the results row (default 4)\n"
             "   -b <Block Dimension>  recorded; the library picks the launch shape\n"
             "   -g <Use Global Mem>   recorded; the library picks shared or global workspaces\n"
-            "   -n <Number of Blocks> recorded; the library sizes the persistent grid\n\n");
+            "   -n <Number of Blocks> recorded; the library sizes the persistent grid\n"
+            "   -z                    vertex ids in the graph file start at 0 (the formated_* inputs)\n\n");
 }
 
 const char *asString(Version v) { return v == STACK_ONLY ? "stackonly" : (v == HYBRID ? "hybrid" : "sequential"); }
@@ -84,7 +86,7 @@ Config parseArgs(int argc, char **argv)
 {
     Config c;
     int opt;
-    while ((opt = getopt(argc, argv, "v:f:o:i:k:q:t:d:b:g:n:h")) >= 0) {
+    while ((opt = getopt(argc, argv, "v:f:o:i:k:q:t:d:b:g:n:hz")) >= 0) {
         switch (opt) {
         case 'v':
             if (!strcmp(optarg, "stackonly")) c.version = STACK_ONLY;
@@ -106,6 +108,7 @@ Config parseArgs(int argc, char **argv)
         case 'b': c.blockDim = (unsigned)atoi(optarg); break;
         case 'g': c.userDefMemory = true; c.useGlobalMemory = atoi(optarg) != 0; break;
         case 'n': c.numBlocks = (unsigned)atoi(optarg); break;
+        case 'z': c.zeroBased = true; break;
         case 'h': usage(); exit(0);
         default: fprintf(stderr, "\nUnrecognized option!\n"); exit(0);
         }
@@ -113,10 +116,12 @@ Config parseArgs(int argc, char **argv)
     return c;
 }
 
-// Reads "n m" and m 1-based edges into a CSR with sorted rows; false + message
-// on any malformed input.
-bool loadGraph(const char *path, uint32_t &n, uint32_t &m, std::vector<uint32_t> &rp, std::vector<uint32_t> &col,
-               std::string &err)
+// Reads "n m" and m edges (1-based ids, or 0-based with zero_based) into a
+// CSR with sorted rows; false + message on any malformed input.  One pass over
+// the file, then a sort of each row, which also finds duplicate edges in
+// O(m log d) instead of the reference's O(V^2) check (auxFunctions.cpp:308-354).
+bool loadGraph(const char *path, bool zero_based, uint32_t &n, uint32_t &m, std::vector<uint32_t> &rp,
+               std::vector<uint32_t> &col, std::string &err)
 {
     FILE *f = fopen(path, "rb");
     if (!f) { err = std::string("cannot open ") + path + ": " + strerror(errno); return false; }
@@ -144,10 +149,14 @@ bool loadGraph(const char *path, uint32_t &n, uint32_t &m, std::vector<uint32_t>
     for (uint32_t i = 0; i < m; ++i) {
         unsigned long a, b;
         if (!next(a) || !next(b)) { err = "fewer edges than the header says"; return false; }
-        if (a < 1 || b < 1 || a > n || b > n) { err = "vertex id out of range (ids are 1-based)"; return false; }
+        if (!zero_based && (a < 1 || b < 1 || a > n || b > n)) {
+            err = "vertex id out of range (ids are 1-based; -z reads 0-based files)";
+            return false;
+        }
+        if (zero_based && (a >= n || b >= n)) { err = "vertex id out of range (ids are 0-based with -z)"; return false; }
         if (a == b) { err = "self-loop"; return false; }
-        eu[i] = (uint32_t)(a - 1);
-        ev[i] = (uint32_t)(b - 1);
+        eu[i] = (uint32_t)(zero_based ? a : a - 1);
+        ev[i] = (uint32_t)(zero_based ? b : b - 1);
         ++deg[eu[i]];
         ++deg[ev[i]];
     }
@@ -183,6 +192,53 @@ void printResults(const Config &c, uint32_t n, uint32_t m, unsigned minimum, uns
     fclose(out);
 }
 
+// The file's name without its directories (src/Counters.cuh:63-70).
+std::string baseName(const char *path)
+{
+    std::string p(path);
+    const size_t k = p.find_last_of('/');
+    return k == std::string::npos ? p : p.substr(k + 1);
+}
+
+// With VC_COUNTERS=1 in the environment (the reference's USE_COUNTERS build,
+// src/Counters.cuh:56-135, main.cu:368-371): NODES_PER_SM/NODES_PER_SM_<prefix>_<file>
+// in the reference's layout (a header SM_1..SM_n and one row of tree nodes per
+// SM), and Counters/Counters_<prefix>_<file> with one row per search unit.  The
+// second file keeps the reference's name and CSV form; its columns are this
+// build's counters, because one sweep decides all three reduction rules here
+// (phase cycles need a VC_PHASE_TIMERS=1 build, otherwise they read 0).
+void printCounters(const Config &c, int sms)
+{
+    const uint32_t nsu = vc_debug_stats(0, -1, nullptr, 0, nullptr);
+    std::vector<uint64_t> rows((size_t)nsu * 16);
+    uint32_t shape[5];
+    vc_debug_stats(0, -1, rows.data(), nsu, shape);
+    const std::string tail = std::string(c.outputFilePrefix) + "_" + baseName(c.graphFileName);
+    mkdir("Counters", 0755);
+    if (FILE *f = fopen(("Counters/Counters_" + tail).c_str(), "w")) {
+        fprintf(f, "SU_NO,NODES,PASSES,DONATIONS,DONATE_FAIL,RECEIVES,ROOTS,BUSY_CYCLES,IDLE_CYCLES,POLLS,RESTORED,"
+                   "SMID,SCAN_CYCLES,APPLY_CYCLES,POP_CYCLES,BRANCH_CYCLES\n");
+        for (uint32_t i = 0; i < nsu; ++i) {
+            fprintf(f, "%u", i);
+            for (int j = 0; j < 15; ++j) fprintf(f, ",%llu", (unsigned long long)rows[(size_t)i * 16 + j]);
+            fprintf(f, "\n");
+        }
+        fclose(f);
+    }
+    std::vector<unsigned long long> per_sm(std::max(sms, 1), 0);
+    for (uint32_t i = 0; i < nsu; ++i) {
+        const uint64_t sm = rows[(size_t)i * 16 + 10];
+        if (sm < per_sm.size()) per_sm[sm] += rows[(size_t)i * 16 + 0];
+    }
+    mkdir("NODES_PER_SM", 0755);
+    if (FILE *f = fopen(("NODES_PER_SM/NODES_PER_SM_" + tail).c_str(), "w")) {
+        for (size_t i = 0; i < per_sm.size(); ++i) fprintf(f, "SM_%zu%s", i + 1, i + 1 < per_sm.size() ? "," : "");
+        fprintf(f, "\n");
+        for (size_t i = 0; i < per_sm.size(); ++i) fprintf(f, "%llu%s", per_sm[i], i + 1 < per_sm.size() ? "," : "");
+        fclose(f);
+    }
+}
+
 }  // namespace
 
 int main(int argc, char **argv)
@@ -197,7 +253,7 @@ int main(int argc, char **argv)
     uint32_t n = 0, m = 0;
     std::vector<uint32_t> rp, col;
     std::string err;
-    if (!loadGraph(config.graphFileName, n, m, rp, col, err)) {
+    if (!loadGraph(config.graphFileName, config.zeroBased, n, m, rp, col, err)) {
         fprintf(stderr, "%s: %s\n", config.graphFileName, err.c_str());
         return 1;
     }
@@ -217,6 +273,9 @@ int main(int argc, char **argv)
     vc_result res;
     memset(&res, 0, sizeof(res));
     res.cover_mask = cover.data();
+    const char *counters_env = getenv("VC_COUNTERS");
+    const bool counters = counters_env && counters_env[0] == '1';
+    if (counters) vc_debug_stats(0, 1, nullptr, 0, nullptr);
     vc_status st = vc_solve(&g, &req, &res);
     if (st != VC_OK) {
         fprintf(stderr, "GPU Error: %s\n", vc_status_string(st));
@@ -232,6 +291,7 @@ int main(int argc, char **argv)
     printf("NumOfSearchUnits : %u\n\n", shape[3]);
     printf("Elapsed time: %fms \n", res.kernel_ms);
     printResults(config, n, m, res.size, res.decision, res.kernel_ms, shape, sms);
+    if (counters) printCounters(config, sms);
     if (config.instance == PVC) {
         if (res.decision) printf("\nMinimum is less than or equal to K: %u\n\n", config.k);
         else printf("\nMinimum is greater than K: %u\n\n", config.k);

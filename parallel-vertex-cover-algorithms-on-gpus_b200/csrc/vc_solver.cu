@@ -509,7 +509,9 @@ extern "C" uint32_t vc_debug_stats(int32_t device, int32_t enable, uint64_t *row
     if (enable >= 0) c->force_sparse = (enable & 2) != 0;
     uint32_t nsu = c->last_num_su;
     if (rows) {
+        // rows exist only for a launch that ran with the counters on
         uint32_t k = std::min(nsu, max_rows);
+        k = std::min<uint32_t>(k, (uint32_t)(c->last_stats.size() / kStatWords));
         memcpy(rows, c->last_stats.data(), sizeof(uint64_t) * kStatWords * k);
     }
     if (launch_shape) {

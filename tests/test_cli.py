@@ -47,6 +47,17 @@ def test_malformed_files(tmp_path, body, msg):
 
 
 @needs_cli
+@pytest.mark.parametrize("body", ["3 1\n0 3\n", "3 2\n0 1\n1 1\n"])
+def test_zero_based_mode_checks(tmp_path, body):
+    """-z reads 0-based ids (the formated_* inputs); id n is out of range there,
+    and the other checks still apply."""
+    p = tmp_path / "g0.txt"
+    p.write_text(body)
+    r = run(["-z", "-f", str(p)], tmp_path)
+    assert r.returncode == 1 and ("out of range" in r.stderr or "self-loop" in r.stderr)
+
+
+@needs_cli
 @pytest.mark.gpu
 def test_cli_solves_and_writes_results_row(tmp_path):
     g = W.config1_graph()
@@ -67,3 +78,40 @@ def test_cli_solves_and_writes_results_row(tmp_path):
     assert f[0] == "run7" and f[2] == "60" and f[3] == str(g.m) and f[4] == "mvc" and f[5] == "hybrid"
     assert f[6] == str(1 << 19) and f[18] == str(opt)
     assert rows[1].split(",")[20] == "0" and rows[2].split(",")[20] == "1"
+
+
+@pytest.mark.gpu
+def test_cli_counters_files(tmp_path):
+    """VC_COUNTERS=1 writes the reference's NODES_PER_SM file (SM_1..SM_n header,
+    tree nodes per SM) and a per-search-unit Counters file."""
+    g = W.config1_graph()
+    p = tmp_path / "g60.txt"
+    W.write_reference_file(g, str(p))
+    env = dict(os.environ, VC_COUNTERS="1")
+    r = subprocess.run([CLI, "-f", str(p), "-o", "c1"], cwd=tmp_path, capture_output=True, text=True, env=env,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    nodes = (tmp_path / "NODES_PER_SM" / "NODES_PER_SM_c1_g60.txt").read_text().splitlines()
+    hdr, vals = nodes[0].split(","), [int(x) for x in nodes[1].split(",")]
+    assert hdr[0] == "SM_1" and len(hdr) == len(vals) and len(hdr) >= 100
+    cnt = (tmp_path / "Counters" / "Counters_c1_g60.txt").read_text().splitlines()
+    assert cnt[0].startswith("SU_NO,NODES,")
+    su_nodes = sum(int(l.split(",")[1]) for l in cnt[1:])
+    assert su_nodes == sum(vals) > 0
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_zero_based_file_same_answer(tmp_path):
+    """A graph written with 0-based ids and read with -z gives the same cover
+    size as the 1-based file."""
+    g = W.config1_graph()
+    p1 = tmp_path / "g1.txt"
+    W.write_reference_file(g, str(p1))
+    lines = p1.read_text().strip().splitlines()
+    p0 = tmp_path / "g0.txt"
+    p0.write_text("\n".join([lines[0]] + [" ".join(str(int(x) - 1) for x in l.split()) for l in lines[1:]]) + "\n")
+    opt = O.mvc(g)[1]
+    r = run(["-z", "-f", str(p0)], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert f"Size of minimum vertex cover: {opt}" in r.stdout
