@@ -123,6 +123,20 @@ vc_status vc_solve_batch(const vc_csr_arena *arena, const vc_request *reqs, vc_r
 vc_status vc_solve_batch_device(const vc_csr_arena *arena, const uint32_t *d_row_ptr, const uint32_t *d_col,
                                 const vc_request *reqs, vc_result *out);
 
+/* The reference's upper-bound heuristics on the GPU, one CTA per graph of the
+ * arena (any sizes; host arrays, copied by the call).
+ * vc_remove_max_ub replaces RemoveMaxApproximateMVC (src/auxFunctions.cpp:211-256),
+ * vc_remove_edge_ub replaces RemoveEdgeApproximateMVC (:258-306).  Both return the
+ * same bound as the reference on the same graph: the kernel keeps the reference's
+ * order of deletions, its rule sweeps and the row order its deleteVertex leaves
+ * (CSRGraphRep.cpp:44-62).  The reference draws RemoveEdge's edges with
+ * srand(time(0)); rand(), one value per second of wall time: r is that value.
+ * ub[i] receives graph i's bound; cover (optional) receives n_i bytes per graph,
+ * in arena order, 1 = in the cover; kernel_ms (optional) the kernel time. */
+vc_status vc_remove_max_ub(const vc_csr_arena *arena, int32_t device, uint32_t *ub, uint8_t *cover, float *kernel_ms);
+vc_status vc_remove_edge_ub(const vc_csr_arena *arena, uint32_t r, int32_t device, uint32_t *ub, uint8_t *cover,
+                            float *kernel_ms);
+
 /* Continuous-batching server (no counterpart in the reference).  Persistent
  * kernels admit requests while others run; graphs and search state stay on the
  * device.  mem_budget_bytes bounds the device arenas holding admitted graphs

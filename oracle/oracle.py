@@ -47,6 +47,10 @@ def lib():
         L.oracle_pvc.restype = ctypes.c_int
         L.oracle_greedy_ub.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u8p]
         L.oracle_greedy_ub.restype = ctypes.c_uint32
+        L.oracle_remove_max_ub.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u8p]
+        L.oracle_remove_max_ub.restype = ctypes.c_uint32
+        L.oracle_remove_edge_ub.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _u8p]
+        L.oracle_remove_edge_ub.restype = ctypes.c_uint32
         L.oracle_is_cover.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u8p]
         L.oracle_is_cover.restype = ctypes.c_int
         _lib = L
@@ -69,6 +73,8 @@ def ref():
             fn.restype = ctypes.c_uint32
         L.ref_remove_max_ub.argtypes = [ctypes.c_uint32, _u32p, _u32p]
         L.ref_remove_max_ub.restype = ctypes.c_uint32
+        L.ref_remove_edge_ub.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.POINTER(ctypes.c_uint32)]
+        L.ref_remove_edge_ub.restype = ctypes.c_uint32
         L.ref_load.argtypes = [ctypes.c_char_p, _u32p, _u32p, ctypes.POINTER(_u32p), ctypes.POINTER(_u32p)]
         L.ref_load.restype = ctypes.c_int
         L.ref_free.argtypes = [ctypes.c_void_p]
@@ -143,6 +149,81 @@ def ref_pvc(g, k: int) -> int:
     """The reference's own SequentialParameterized(graph, k+1, k) -> kFound."""
     rp, col = _arrays(g)
     return int(ref().ref_pvc(g.n, _p32(rp), _p32(col), k))
+
+
+def remove_max_ub(g) -> Tuple[int, np.ndarray]:
+    """RemoveMaxApproximateMVC restated exactly (src/auxFunctions.cpp:211-256):
+    (cover size, cover mask)."""
+    rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
+    col = np.ascontiguousarray(g.col, dtype=np.uint32)
+    cover = np.zeros(max(g.n, 1), dtype=np.uint8)
+    ub = int(lib().oracle_remove_max_ub(g.n, _p32(rp), _p32(col), cover.ctypes.data_as(_u8p)))
+    return ub, cover[:g.n].astype(bool)
+
+
+def remove_edge_ub(g, r: int) -> Tuple[int, np.ndarray]:
+    """RemoveEdgeApproximateMVC restated exactly with rand() == r
+    (src/auxFunctions.cpp:258-306): (cover size, cover mask)."""
+    rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
+    col = np.ascontiguousarray(g.col, dtype=np.uint32)
+    cover = np.zeros(max(g.n, 1), dtype=np.uint8)
+    ub = int(lib().oracle_remove_edge_ub(g.n, _p32(rp), _p32(col), r, cover.ctypes.data_as(_u8p)))
+    return ub, cover[:g.n].astype(bool)
+
+
+def ref_remove_edge_ub_forked(g) -> Optional[Tuple[int, int]]:
+    """The reference's own RemoveEdgeApproximateMVC in a forked child: (bound,
+    the rand() value its calls used), or None if the run crossed a second
+    boundary or the child failed."""
+    r, w = os.pipe()
+    pid = os.fork()
+    if pid == 0:
+        os.close(r)
+        try:
+            rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
+            col = np.ascontiguousarray(g.col, dtype=np.uint32)
+            ro = ctypes.c_uint32(0)
+            v = ref().ref_remove_edge_ub(g.n, _p32(rp), _p32(col), ctypes.byref(ro))
+            os.write(w, f"{v} {ro.value}".encode())
+        finally:
+            os._exit(0)
+    os.close(w)
+    data = b""
+    while True:
+        chunk = os.read(r, 64)
+        if not chunk:
+            break
+        data += chunk
+    os.close(r)
+    _, status = os.waitpid(pid, 0)
+    if not data or status != 0:
+        return None
+    v, rv = (int(x) for x in data.split())
+    return None if v == 0xFFFFFFFF else (v, rv)
+
+
+def ref_remove_max_ub_forked(g) -> Optional[int]:
+    """The reference's own RemoveMaxApproximateMVC in a forked child (its binary
+    search can read out of bounds on rare inputs); None if the child failed."""
+    r, w = os.pipe()
+    pid = os.fork()
+    if pid == 0:
+        os.close(r)
+        try:
+            v = ref_remove_max_ub(g)
+            os.write(w, str(v).encode())
+        finally:
+            os._exit(0)
+    os.close(w)
+    data = b""
+    while True:
+        chunk = os.read(r, 64)
+        if not chunk:
+            break
+        data += chunk
+    os.close(r)
+    _, status = os.waitpid(pid, 0)
+    return int(data) if data and status == 0 else None
 
 
 def ref_remove_max_ub(g) -> int:

@@ -14,6 +14,8 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <ctime>
+#include <cstdlib>
 #include "CSRGraphRep.h"
 #include "Sequential.h"
 #include "SequentialParameterized.h"
@@ -51,6 +53,23 @@ extern "C" uint32_t ref_remove_max_ub(uint32_t n, const uint32_t *row_ptr, const
     CSRGraph g = make_graph(n, row_ptr, col);
     uint32_t ub = RemoveMaxApproximateMVC(g);
     g.del();
+    return ub;
+}
+
+// RemoveEdgeApproximateMVC(graph) (src/auxFunctions.cpp:258), which draws its
+// edges with srand(time(0)); rand() on every call.  When the run starts and ends
+// in the same second, *r_out receives the value those calls returned and the
+// bound is returned; otherwise UINT32_MAX.
+extern "C" uint32_t ref_remove_edge_ub(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint32_t *r_out)
+{
+    CSRGraph g = make_graph(n, row_ptr, col);
+    const time_t t0 = time(0);
+    uint32_t ub = RemoveEdgeApproximateMVC(g);
+    const time_t t1 = time(0);
+    g.del();
+    if (t0 != t1) return UINT32_MAX;
+    srand((unsigned)t0);
+    *r_out = (uint32_t)rand();
     return ub;
 }
 

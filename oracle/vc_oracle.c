@@ -18,6 +18,12 @@
  *   greedy UB   -> the "always take the max-degree vertex" descent of
  *                  src/auxFunctions.cpp:211-256 (RemoveMaxApproximateMVC), stated on
  *                  the degree-array state (see oracle_greedy_ub below).
+ *   oracle_remove_max_ub -> RemoveMaxApproximateMVC exactly (src/auxFunctions.cpp:
+ *                  44-127, 211-256 with CSRGraph::deleteVertex, CSRGraphRep.cpp:44-62):
+ *                  rows are compacted on deletion and the triangle test binary-searches
+ *                  the compacted (unsorted) row, as the reference does.
+ *   oracle_remove_edge_ub -> RemoveEdgeApproximateMVC exactly (auxFunctions.cpp:258-306),
+ *                  with the value rand() returns after srand(time(0)) as a parameter.
  *
  * Same rules, same order (leaf, triangle, high-degree; repeat while triangle or
  * high-degree changed), same branching (max-degree vertex, lowest index on ties;
@@ -297,6 +303,177 @@ uint32_t oracle_greedy_ub(uint32_t n, const uint32_t *row_ptr, const uint32_t *c
     if (cover_out) for (uint32_t i = 0; i < n; ++i) cover_out[i] = deg[i] == -1;
     free(deg);
     return del;
+}
+
+/* RemoveMaxApproximateMVC (src/auxFunctions.cpp:211-256) restated exactly on a
+ * working copy of the CSR that deletions compact, as CSRGraph::deleteVertex
+ * does (CSRGraphRep.cpp:44-62): deleting v takes v out of the live prefix of
+ * each live neighbour's row by copying that row's last live entry over it.
+ * One iteration runs the leaf rule to a fixpoint (auxFunctions.cpp:44-69: passes
+ * over the vertices in index order while a pass met a degree-1 vertex), then
+ * the triangle rule to a fixpoint (:71-127: the first degree-2 vertex whose two
+ * live neighbours pass the keep test and are found adjacent by a binary search
+ * of the second neighbour's whole, compacted row; restart from vertex 0), then
+ * deletes the lowest-index vertex of maximum degree; both rules return false, so
+ * the do-while of :222-231 runs once.  The binary search (:25-42) is the same
+ * except that where the reference's unsigned index would step below 0 (and read
+ * out of bounds) this one stops with "not found".  Returns the cover size; the
+ * cover (vertices deleted) goes to cover_out when non-null. */
+static void rm_delete(const uint32_t *rp, uint32_t *dst, int32_t *deg, uint32_t v)
+{
+    const uint32_t b = rp[v], e = b + (uint32_t)deg[v];
+    for (uint32_t i = b; i < e; ++i) {
+        const uint32_t w = dst[i];
+        const uint32_t last = rp[w] + (uint32_t)deg[w];
+        for (uint32_t j = rp[w]; j < last; ++j) {
+            if (dst[j] == v) {
+                dst[j] = dst[last - 1];
+                if (deg[w] != -1) --deg[w];
+            }
+        }
+    }
+    deg[v] = -1;
+}
+
+static int rm_search(const uint32_t *arr, long l, long r, uint32_t x)
+{
+    while (l <= r) {
+        const long m = l + (r - l) / 2;
+        if (arr[m] == x) return 1;
+        if (arr[m] < x) l = m + 1;
+        else r = m - 1;
+    }
+    return 0;
+}
+
+uint32_t oracle_remove_max_ub(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint8_t *cover_out)
+{
+    const uint32_t m2 = row_ptr[n];
+    uint32_t *dst = (uint32_t *)malloc((size_t)(m2 ? m2 : 1) * sizeof(uint32_t));
+    int32_t *deg = (int32_t *)malloc((size_t)(n ? n : 1) * sizeof(int32_t));
+    if (!dst || !deg) { free(dst); free(deg); return n; }
+    memcpy(dst, col, (size_t)m2 * sizeof(uint32_t));
+    for (uint32_t v = 0; v < n; ++v) deg[v] = (int32_t)(row_ptr[v + 1] - row_ptr[v]);
+    uint32_t minimum = 0;
+    for (;;) {
+        int changed;
+        do {  /* leaf rule */
+            changed = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                if (deg[i] != 1) continue;
+                changed = 1;
+                for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j)
+                    if (deg[dst[j]] != -1) { rm_delete(row_ptr, dst, deg, dst[j]); ++minimum; }
+            }
+        } while (changed);
+        do {  /* triangle rule */
+            changed = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                if (deg[i] != 2) continue;
+                uint32_t n1 = 0, n2 = 0;
+                int found1 = 0, keep = 0;
+                for (uint32_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+                    const uint32_t u = dst[e];
+                    const int32_t du = deg[u];
+                    if (du > 0) {
+                        if (du == 1 || (du == 2 && u < i)) { keep = 1; break; }
+                        else if (!found1) { found1 = 1; n1 = u; }
+                        else { n2 = u; break; }
+                    }
+                }
+                if (!keep && rm_search(dst, (long)row_ptr[n2], (long)row_ptr[n2 + 1] - 1, n1)) {
+                    rm_delete(row_ptr, dst, deg, n1);
+                    rm_delete(row_ptr, dst, deg, n2);
+                    minimum += 2;
+                    changed = 1;
+                    break;
+                }
+            }
+        } while (changed);
+        uint32_t maxv = 0;
+        int32_t maxd = 0;
+        for (uint32_t i = 0; i < n; ++i)
+            if (deg[i] > maxd) { maxv = i; maxd = deg[i]; }
+        if (maxd == 0) break;
+        rm_delete(row_ptr, dst, deg, maxv);
+        ++minimum;
+    }
+    if (cover_out) for (uint32_t i = 0; i < n; ++i) cover_out[i] = deg[i] == -1;
+    free(dst);
+    free(deg);
+    return minimum;
+}
+
+/* RemoveEdgeApproximateMVC (src/auxFunctions.cpp:258-306) restated exactly,
+ * on the same compacting CSR copy as oracle_remove_max_ub.  For each vertex in
+ * index order, while the running edge count is positive: the leaf rule and the
+ * triangle rule to their fixpoints (the do-while runs once, both rules return
+ * false), then, if the vertex still has live neighbours, it and the neighbour at
+ * row position (r mod degree) of its compacted row go into the cover.  The
+ * reference draws that position with srand(time(0)); rand() on every call
+ * (getRandom, :251-256), i.e. one value r for all calls within one second; here r
+ * is a parameter.  The edge count is decremented only for the pair taken, as in
+ * the reference (unsigned arithmetic).  Returns the cover size. */
+uint32_t oracle_remove_edge_ub(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint32_t r,
+                               uint8_t *cover_out)
+{
+    const uint32_t m2 = row_ptr[n];
+    uint32_t *dst = (uint32_t *)malloc((size_t)(m2 ? m2 : 1) * sizeof(uint32_t));
+    int32_t *deg = (int32_t *)malloc((size_t)(n ? n : 1) * sizeof(int32_t));
+    if (!dst || !deg) { free(dst); free(deg); return n; }
+    memcpy(dst, col, (size_t)m2 * sizeof(uint32_t));
+    for (uint32_t v = 0; v < n; ++v) deg[v] = (int32_t)(row_ptr[v + 1] - row_ptr[v]);
+    uint32_t minimum = 0, remaining = m2 / 2;
+    for (uint32_t vertex = 0; vertex < n && remaining > 0; ++vertex) {
+        int changed;
+        do {  /* leaf rule */
+            changed = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                if (deg[i] != 1) continue;
+                changed = 1;
+                for (uint32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j)
+                    if (deg[dst[j]] != -1) { rm_delete(row_ptr, dst, deg, dst[j]); ++minimum; }
+            }
+        } while (changed);
+        do {  /* triangle rule */
+            changed = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                if (deg[i] != 2) continue;
+                uint32_t n1 = 0, n2 = 0;
+                int found1 = 0, keep = 0;
+                for (uint32_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+                    const uint32_t u = dst[e];
+                    const int32_t du = deg[u];
+                    if (du > 0) {
+                        if (du == 1 || (du == 2 && u < i)) { keep = 1; break; }
+                        else if (!found1) { found1 = 1; n1 = u; }
+                        else { n2 = u; break; }
+                    }
+                }
+                if (!keep && rm_search(dst, (long)row_ptr[n2], (long)row_ptr[n2 + 1] - 1, n1)) {
+                    rm_delete(row_ptr, dst, deg, n1);
+                    rm_delete(row_ptr, dst, deg, n2);
+                    minimum += 2;
+                    changed = 1;
+                    break;
+                }
+            }
+        } while (changed);
+        if (deg[vertex] > 0) {
+            const uint32_t e = row_ptr[vertex] + r % (uint32_t)deg[vertex];
+            const uint32_t u = dst[e];
+            remaining -= (uint32_t)deg[vertex];
+            remaining -= (uint32_t)deg[u];
+            ++remaining;
+            rm_delete(row_ptr, dst, deg, vertex);
+            rm_delete(row_ptr, dst, deg, u);
+            minimum += 2;
+        }
+    }
+    if (cover_out) for (uint32_t i = 0; i < n; ++i) cover_out[i] = deg[i] == -1;
+    free(dst);
+    free(deg);
+    return minimum;
 }
 
 /* Edge-by-edge check: 1 iff every edge has an endpoint with cover[v] != 0. */

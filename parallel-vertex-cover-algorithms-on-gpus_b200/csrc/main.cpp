@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <ctime>
 #include <string>
 #include <vector>
 
@@ -57,6 +58,7 @@ struct Config {
     const char *outputFilePrefix = "1";
     const char *graphFileName = "GraphInput.txt";
     bool zeroBased = false;  // -z: vertex ids in the file start at 0
+    bool upperBounds = false;  // -u: the reference's two upper-bound heuristics, on the GPU
 };
 
 void usage()
@@ -76,7 +78,8 @@ void usage()
             "   -b <Block Dimension>  recorded; the library picks the launch shape\n"
             "   -g <Use Global Mem>   recorded; the library picks shared or global workspaces\n"
             "   -n <Number of Blocks> recorded; the library sizes the persistent grid\n"
-            "   -z                    vertex ids in the graph file start at 0 (the formated_* inputs)\n\n");
+            "   -z                    vertex ids in the graph file start at 0 (the formated_* inputs)\n"
+            "   -u                    also run the RemoveMax / RemoveEdge upper-bound heuristics (on the GPU)\n\n");
 }
 
 const char *asString(Version v) { return v == STACK_ONLY ? "stackonly" : (v == HYBRID ? "hybrid" : "sequential"); }
@@ -86,7 +89,7 @@ Config parseArgs(int argc, char **argv)
 {
     Config c;
     int opt;
-    while ((opt = getopt(argc, argv, "v:f:o:i:k:q:t:d:b:g:n:hz")) >= 0) {
+    while ((opt = getopt(argc, argv, "v:f:o:i:k:q:t:d:b:g:n:hzu")) >= 0) {
         switch (opt) {
         case 'v':
             if (!strcmp(optarg, "stackonly")) c.version = STACK_ONLY;
@@ -109,6 +112,7 @@ Config parseArgs(int argc, char **argv)
         case 'g': c.userDefMemory = true; c.useGlobalMemory = atoi(optarg) != 0; break;
         case 'n': c.numBlocks = (unsigned)atoi(optarg); break;
         case 'z': c.zeroBased = true; break;
+        case 'u': c.upperBounds = true; break;
         case 'h': usage(); exit(0);
         default: fprintf(stderr, "\nUnrecognized option!\n"); exit(0);
         }
@@ -176,8 +180,13 @@ bool loadGraph(const char *path, bool zero_based, uint32_t &n, uint32_t &m, std:
     return true;
 }
 
+struct Bounds {
+    unsigned maxApprox = 0, edgeApprox = 0;
+    double timeMax = 0, timeEdge = 0;  // seconds
+};
+
 void printResults(const Config &c, uint32_t n, uint32_t m, unsigned minimum, unsigned kFound, float ms,
-                  const uint32_t *shape, int sms)
+                  const uint32_t *shape, int sms, const Bounds &b)
 {
     mkdir("Results", 0755);
     FILE *out = fopen("Results/Results.csv", "a");
@@ -188,7 +197,7 @@ void printResults(const Config &c, uint32_t n, uint32_t m, unsigned minimum, uns
     fprintf(out, "%s,%s,%u,%u,%s,%s,%d,%f,%d,%d,%d,%u,%d,%d,%u,%f,%u,%f,%u,%u,%u,%f\n", c.outputFilePrefix,
             c.graphFileName, n, m, asString(c.instance), asString(c.version), (int)c.globalListSize,
             c.globalListThreshold, (int)c.startingDepth, useGlobal, (int)block, per_sm, (int)(per_sm * block),
-            (int)grid, 0u, 0.0, 0u, 0.0, minimum, c.k, kFound, ms);
+            (int)grid, b.maxApprox, b.timeMax, b.edgeApprox, b.timeEdge, minimum, c.k, kFound, ms);
     fclose(out);
 }
 
@@ -263,6 +272,36 @@ int main(int argc, char **argv)
     g.row_ptr = rp.data();
     g.col = col.empty() ? nullptr : col.data();
     g.degree = nullptr;
+    Bounds bounds;
+    if (config.upperBounds) {  // main.cu:55-74 of the reference, with both heuristics on the GPU
+        const uint64_t zero = 0;
+        vc_csr_arena a;
+        a.count = 1;
+        a.n = &n;
+        a.row_off = &zero;
+        a.col_off = &zero;
+        a.row_ptr = rp.data();
+        a.col = col.empty() ? nullptr : col.data();
+        float ms = 0;
+        // rand() right after srand(time(0)), the value the reference's draws use
+        srand((unsigned)time(nullptr));
+        const uint32_t r = (uint32_t)rand();
+        if (vc_remove_max_ub(&a, 0, &bounds.maxApprox, nullptr, &ms) != VC_OK) {
+            fprintf(stderr, "GPU Error: RemoveMax upper bound\n");
+            return 1;
+        }
+        bounds.timeMax = ms / 1e3;
+        printf("\nElapsed Time for Approximate Remove Max: %f\n", bounds.timeMax);
+        printf("Approximate Remove Max Minimum is: %u\n", bounds.maxApprox);
+        if (vc_remove_edge_ub(&a, r, 0, &bounds.edgeApprox, nullptr, &ms) != VC_OK) {
+            fprintf(stderr, "GPU Error: RemoveEdge upper bound\n");
+            return 1;
+        }
+        bounds.timeEdge = ms / 1e3;
+        printf("Elapsed Time for Approximate Remove Edge: %f\n", bounds.timeEdge);
+        printf("Approximate Remove Edge Minimum is: %u\n", bounds.edgeApprox);
+        fflush(stdout);
+    }
     vc_request req;
     memset(&req, 0, sizeof(req));
     req.instance = config.instance == PVC ? VC_PVC : VC_MVC;
@@ -290,7 +329,7 @@ int main(int argc, char **argv)
     printf("NumOfBlocks : %u\n", shape[0]);
     printf("NumOfSearchUnits : %u\n\n", shape[3]);
     printf("Elapsed time: %fms \n", res.kernel_ms);
-    printResults(config, n, m, res.size, res.decision, res.kernel_ms, shape, sms);
+    printResults(config, n, m, res.size, res.decision, res.kernel_ms, shape, sms, bounds);
     if (counters) printCounters(config, sms);
     if (config.instance == PVC) {
         if (res.decision) printf("\nMinimum is less than or equal to K: %u\n\n", config.k);

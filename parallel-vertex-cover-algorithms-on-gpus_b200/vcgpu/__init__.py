@@ -105,6 +105,12 @@ def lib():
             L.vc_server_submit.restype = ctypes.c_int
             L.vc_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]
             L.vc_server_poll.restype = ctypes.c_int
+            L.vc_remove_max_ub.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_float)]
+            L.vc_remove_max_ub.restype = ctypes.c_int
+            L.vc_remove_edge_ub.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
+            L.vc_remove_edge_ub.restype = ctypes.c_int
             L.vc_server_completed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                               ctypes.POINTER(ctypes.c_uint32)]
             L.vc_server_completed.restype = ctypes.c_int
@@ -234,6 +240,46 @@ def debug_stats(enable: Optional[bool] = None, device: int = -1):
     rows = np.zeros((max(nsu, 1), 16), dtype=np.uint64)
     L.vc_debug_stats(device, -1, rows.ctypes.data, nsu, shape.ctypes.data)
     return rows[:nsu], shape
+
+
+def _ub(kind: str, arena, r: int, device: int):
+    if not hasattr(arena, "row_off"):  # one Graph
+        from . import workloads
+        arena = workloads.pack([arena])
+    n = np.ascontiguousarray(arena.n, dtype=np.uint32)
+    ro = np.ascontiguousarray(arena.row_off, dtype=np.uint64)
+    co = np.ascontiguousarray(arena.col_off, dtype=np.uint64)
+    rp = np.ascontiguousarray(arena.row_ptr, dtype=np.uint32)
+    col = np.ascontiguousarray(arena.col, dtype=np.uint32)
+    a = CsrArena(arena.count, n.ctypes.data, ro.ctypes.data, co.ctypes.data, rp.ctypes.data,
+                 col.ctypes.data if col.size else None)
+    ub = np.zeros(max(arena.count, 1), dtype=np.uint32)
+    cover = np.zeros(max(int(n.sum()), 1), dtype=np.uint8)
+    ms = ctypes.c_float(0.0)
+    if kind == "max":
+        st = lib().vc_remove_max_ub(ctypes.byref(a), device, ub.ctypes.data, cover.ctypes.data, ctypes.byref(ms))
+    else:
+        st = lib().vc_remove_edge_ub(ctypes.byref(a), r, device, ub.ctypes.data, cover.ctypes.data,
+                                     ctypes.byref(ms))
+    if st != VC_OK:
+        raise RuntimeError(f"vc_remove_{kind}_ub failed: {STATUS_NAMES.get(st, st)}")
+    covers, k = [], 0
+    for ni in n:
+        covers.append(cover[k:k + int(ni)].astype(bool))
+        k += int(ni)
+    return [int(x) for x in ub[:arena.count]], covers, float(ms.value)
+
+
+def remove_max_ub(arena, device: int = -1):
+    """RemoveMaxApproximateMVC on the GPU for every graph of an Arena (or one
+    Graph): (bounds, covers, kernel ms)."""
+    return _ub("max", arena, 0, device)
+
+
+def remove_edge_ub(arena, r: int, device: int = -1):
+    """RemoveEdgeApproximateMVC on the GPU with rand() == r: (bounds, covers,
+    kernel ms)."""
+    return _ub("edge", arena, r, device)
 
 
 def kernel_launches() -> int:

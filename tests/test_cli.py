@@ -115,3 +115,21 @@ def test_cli_zero_based_file_same_answer(tmp_path):
     r = run(["-z", "-f", str(p0)], tmp_path)
     assert r.returncode == 0, r.stderr
     assert f"Size of minimum vertex cover: {opt}" in r.stdout
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_upper_bounds(tmp_path):
+    """-u runs both of the reference's upper-bound heuristics on the GPU, prints
+    their lines and fills the Results.csv fields the fork leaves at zero."""
+    g = W.config1_graph()
+    p = tmp_path / "g60.txt"
+    W.write_reference_file(g, str(p))
+    r = run(["-u", "-f", str(p), "-o", "u1"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    want = O.remove_max_ub(g)[0]
+    assert f"Approximate Remove Max Minimum is: {want}" in r.stdout
+    edge = int(r.stdout.split("Approximate Remove Edge Minimum is: ")[1].split()[0])
+    assert edge >= O.mvc(g)[1]
+    f = (tmp_path / "Results" / "Results.csv").read_text().strip().splitlines()[-1].split(",")
+    assert f[14] == str(want) and f[16] == str(edge)

@@ -124,3 +124,28 @@ def test_greedy_ub_is_a_cover():
         g = W.gnp(80, 0.08, seed)
         ub, cover = O.greedy_ub(g)
         assert O.is_cover(g, cover) and int(cover.sum()) == ub
+
+
+@needs_ref
+def test_upper_bound_restatements_match_reference():
+    """oracle.remove_max_ub / remove_edge_ub restate the reference's
+    RemoveMaxApproximateMVC / RemoveEdgeApproximateMVC exactly: the same bound as
+    the reference's own compiled functions (run in a forked child; for RemoveEdge
+    with the rand() value the reference's run used)."""
+    compared = 0
+    for i in range(120):
+        rng = np.random.default_rng(i)
+        n = int(rng.integers(5, 250))
+        d = float(rng.uniform(1.5, 10))
+        g = W.gnp(n, min(1.0, d / max(n - 1, 1)), 1000 + i) if i % 3 else W.random_regular(n + (n % 2), 3, i)
+        ub, cover = O.remove_max_ub(g)
+        assert W.is_cover(g, cover) and int(cover.sum()) == ub
+        r = O.ref_remove_max_ub_forked(g)
+        assert r is None or r == ub, (g.name, ub, r)
+        res = O.ref_remove_edge_ub_forked(g)
+        if res is not None:
+            ub_e, cover_e = O.remove_edge_ub(g, res[1])
+            assert ub_e == res[0], (g.name, ub_e, res)
+            assert W.is_cover(g, cover_e) and int(cover_e.sum()) == ub_e
+            compared += 1
+    assert compared >= 100
