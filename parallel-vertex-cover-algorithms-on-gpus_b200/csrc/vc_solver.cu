@@ -62,6 +62,9 @@ __global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Param
 #ifndef VC_DENSE8_THREADS
 #define VC_DENSE8_THREADS 1280
 #endif
+#ifndef VC_DENSE_WARPS
+#define VC_DENSE_WARPS 8
+#endif
 #ifndef VC_DENSE4_THREADS
 #define VC_DENSE4_THREADS 1536
 #endif
@@ -239,7 +242,7 @@ static cudaError_t plan_dense(Ctx &c, Plan &pl)
     pl.su_bytes = dense_workspace_bytes(NW);
     pl.stride = (4 + NW + 3) / 4 * 4;
     const uint32_t budget = (uint32_t)c.smem_optin - 1024;
-    uint32_t warps = 8;
+    uint32_t warps = VC_DENSE_WARPS;  // search units sharing one staged graph
     while (warps > 1 && dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget)
         warps >>= 1;
     pl.cta_slots = warps > 1 ? 2 * warps : 0;
