@@ -286,3 +286,15 @@ def test_wide_range_with_a_high_degree_vertex_takes_csr():
     _, shape = vcgpu.debug_stats()
     assert int(shape[4]) >> 31 == 0, shape  # CSR plan
     _check_mvc(g, r, opt)
+
+
+def test_batch_pvc_vs_golden():
+    """Batched PVC over 256 graphs of the batched workload, half at k = opt (yes,
+    with a cover of at most k) and half at k = opt - 1 (no), in one launch."""
+    recs = _golden_batch(2_000_000)[256:512]
+    graphs = [W.batch_instance(r["i"]) for r in recs]
+    ks = [r["opt"] - (j % 2) for j, r in enumerate(recs)]
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "pvc", ks=ks, time_limit=TL)
+    assert st == vcgpu.VC_OK
+    for g, r, rec, k in zip(graphs, sols, recs, ks):
+        _check_pvc(g, r, k, 1 if rec["opt"] <= k else 0)
