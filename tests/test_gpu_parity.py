@@ -298,3 +298,18 @@ def test_batch_pvc_vs_golden():
     assert st == vcgpu.VC_OK
     for g, r, rec, k in zip(graphs, sols, recs, ks):
         _check_pvc(g, r, k, 1 if rec["opt"] <= k else 0)
+
+
+def test_every_golden_batch_graph_up_to_2m_oracle_nodes():
+    """Every graph of the batched workload that the oracle solved within 2 M
+    nodes (most of the 4096), in batches of 1024, without a node budget: the
+    optimum and a verified cover of that size for each."""
+    recs = _golden_batch(2_000_000)
+    assert len(recs) > 3000
+    for c in range(0, len(recs), 1024):
+        chunk = recs[c:c + 1024]
+        graphs = [W.batch_instance(r["i"]) for r in chunk]
+        st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+        assert st == vcgpu.VC_OK
+        for g, r, rec in zip(graphs, sols, chunk):
+            _check_mvc(g, r, rec["opt"])
