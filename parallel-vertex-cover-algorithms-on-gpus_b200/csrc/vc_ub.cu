@@ -66,12 +66,29 @@ struct UbParams {
     uint32_t r;        // RemoveEdge: the value of rand() the reference's draws used
 };
 
+constexpr uint32_t kHubDeg = 128;  // rows longer than this are updated by the whole block
+constexpr uint32_t kHubList = 2048;
+
 struct UbShared {
     uint32_t found;      // block search result
     uint32_t cnt1;       // vertices of degree 1
     uint32_t dirty_any;  // dirty bitmap not empty
+    uint32_t nhub;       // long rows left for the block in this deletion
     unsigned long long amax;  // argmax key: degree << 32 | ~index
+    uint32_t hub[kHubList];
 };
+
+// Bookkeeping after w lost one live neighbour (its degree went from dw to dw-1).
+__device__ __forceinline__ void ub_lost_one(uint32_t *d1, UbShared &sh, uint32_t w, int dw)
+{
+    if (dw - 1 == 1) {
+        atomicOr(&d1[w >> 5], 1u << (w & 31u));
+        atomicAdd(&sh.cnt1, 1u);
+    } else if (dw == 1) {
+        atomicAnd(&d1[w >> 5], ~(1u << (w & 31u)));
+        atomicSub(&sh.cnt1, 1u);
+    }
+}
 
 // Deletes live vertex x (CSRGraph::deleteVertex): each live neighbour w takes
 // x out of its live prefix by moving its last live entry over it.  One thread
@@ -79,23 +96,24 @@ struct UbShared {
 __device__ void ub_delete(const uint32_t *rp, uint32_t *dst, int32_t *deg, uint32_t *d1, uint32_t *dt, UbShared &sh,
                           uint32_t x)
 {
-    __syncthreads();
+    __syncthreads();  // sh.nhub is 0 here: set at the end of the previous deletion and at the start
     const int dx = deg[x];
     for (int t = (int)threadIdx.x; t < dx; t += (int)blockDim.x) {
         const uint32_t w = dst[rp[x] + (uint32_t)t];
         const int dw = deg[w];
+        if ((uint32_t)dw > kHubDeg) {  // a long row: the whole block takes it below
+            const uint32_t slot = atomicAdd(&sh.nhub, 1u);
+            if (slot < kHubList) {
+                sh.hub[slot] = w;
+                continue;
+            }
+        }
         const uint32_t last = rp[w] + (uint32_t)dw;
         for (uint32_t j = rp[w]; j < last; ++j)
             if (dst[j] == x) dst[j] = dst[last - 1];
         const int nd = dw - 1;
         deg[w] = nd;
-        if (nd == 1) {
-            atomicOr(&d1[w >> 5], 1u << (w & 31u));
-            atomicAdd(&sh.cnt1, 1u);
-        } else if (dw == 1) {
-            atomicAnd(&d1[w >> 5], ~(1u << (w & 31u)));
-            atomicSub(&sh.cnt1, 1u);
-        }
+        ub_lost_one(d1, sh, w, dw);
         atomicOr(&dt[w >> 5], 1u << (w & 31u));
         for (uint32_t k = rp[w]; k < rp[w] + (uint32_t)nd; ++k) {
             const uint32_t y = dst[k];
@@ -104,12 +122,41 @@ __device__ void ub_delete(const uint32_t *rp, uint32_t *dst, int32_t *deg, uint3
         sh.dirty_any = 1u;
     }
     __syncthreads();
+    // Long rows, one at a time: the block finds x in w's live prefix, one
+    // thread moves the last live entry over it, the block marks w's neighbours.
+    // Each row is changed exactly as the serial loop above would change it.
+    const uint32_t nhub = min(sh.nhub, kHubList);
+    for (uint32_t h = 0; h < nhub; ++h) {
+        const uint32_t w = sh.hub[h];
+        const int dw = deg[w];
+        const uint32_t b = rp[w], last = b + (uint32_t)dw;
+        if (threadIdx.x == 0) sh.found = kInf;
+        __syncthreads();
+        for (uint32_t j = b + threadIdx.x; j < last; j += blockDim.x)
+            if (dst[j] == x) atomicMin(&sh.found, j);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t j = sh.found;
+            if (j != kInf) dst[j] = dst[last - 1];
+            deg[w] = dw - 1;
+            ub_lost_one(d1, sh, w, dw);
+            atomicOr(&dt[w >> 5], 1u << (w & 31u));
+            sh.dirty_any = 1u;
+        }
+        __syncthreads();
+        for (uint32_t k = b + threadIdx.x; k < b + (uint32_t)(dw - 1); k += blockDim.x) {
+            const uint32_t y = dst[k];
+            atomicOr(&dt[y >> 5], 1u << (y & 31u));
+        }
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         if (deg[x] == 1) {
             atomicAnd(&d1[x >> 5], ~(1u << (x & 31u)));
             sh.cnt1 -= 1u;
         }
         deg[x] = -1;
+        sh.nhub = 0;
     }
     __syncthreads();
 }
@@ -180,6 +227,7 @@ __global__ void __launch_bounds__(kUbThreads) k_ub(UbParams P)
     if (threadIdx.x == 0) {
         sh.cnt1 = 0;
         sh.dirty_any = 1;
+        sh.nhub = 0;
     }
     for (uint32_t e = threadIdx.x; e < m2; e += blockDim.x) dst[e] = col[e];
     for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
