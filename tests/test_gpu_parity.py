@@ -313,3 +313,38 @@ def test_every_golden_batch_graph_up_to_2m_oracle_nodes():
         assert st == vcgpu.VC_OK
         for g, r, rec in zip(graphs, sols, chunk):
             _check_mvc(g, r, rec["opt"])
+
+
+def test_device_input_entry_points():
+    """vc_solve with VC_FLAG_DEVICE_INPUT and vc_solve_batch_device (the CSR
+    already in device memory): the same optima as the host entry points, on an
+    arena that takes every kernel class (dense, wide dense, warp CSR, CTA CSR)."""
+    torch = pytest.importorskip("torch")
+    recs = _golden_batch(200_000)[:40]
+    graphs = [W.batch_instance(r["i"]) for r in recs]
+    opts = [r["opt"] for r in recs]
+    wide = _wide_graphs()[:4]
+    graphs += [g for g, _ in wide]
+    opts += [o for _, o in wide]
+    rng = np.random.default_rng(313)
+    for n in (900, 1500):
+        g = W.gnp(n, 2.2 / (n - 1), int(rng.integers(1 << 30)))
+        st, opt, _, _ = O.mvc(g, node_limit=2_000_000)
+        assert st == O.OK
+        graphs.append(g)
+        opts.append(opt)
+    arena = W.pack(graphs)
+    d_rp = torch.from_numpy(arena.row_ptr.astype(np.int32)).cuda()
+    d_col = torch.from_numpy(arena.col.astype(np.int32)).cuda()
+    torch.cuda.synchronize()
+    st, sols = vcgpu.solve_batch(arena, "mvc", time_limit=TL, d_row_ptr=d_rp.data_ptr(), d_col=d_col.data_ptr())
+    assert st == vcgpu.VC_OK
+    for g, r, opt in zip(graphs, sols, opts):
+        _check_mvc(g, r, opt)
+    for j in (0, 40, len(graphs) - 1):  # one graph at a time, device-resident
+        g = graphs[j]
+        grp = torch.from_numpy(g.row_ptr.astype(np.int32)).cuda()
+        gcol = torch.from_numpy(g.col.astype(np.int32)).cuda()
+        torch.cuda.synchronize()
+        r = vcgpu.solve_device(g.n, g.m, grp.data_ptr(), gcol.data_ptr(), "mvc", time_limit=TL)
+        _check_mvc(g, r, opts[j])
