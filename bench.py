@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=128)
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--ref-step-s", type=float, default=30.0)
-    ap.add_argument("--workload", default="batch", choices=["batch", "stream"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub"])
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--stream-seconds", type=float, default=60.0)
     ap.add_argument("--stream-max-vertices", type=int, default=0)
@@ -429,6 +429,44 @@ def stream_arm(args, world, rank):
     print(json.dumps(line))
 
 
+def ub_arm(args, world, rank):
+    """The reference's upper-bound heuristics on the GPU (vc_remove_max_ub /
+    vc_remove_edge_ub): Chung-Lu n=100000 (one graph) and the 4096 batched
+    graphs, beside the reference's own CPU functions on the Chung-Lu graph
+    (forked child, one core).  rand() value 12345 for RemoveEdge."""
+    if rank != 0:
+        return
+    import vcgpu
+    g5 = W.chung_lu()
+    arena = W.pack(W.batch_graphs(args.count, seed=0))
+    r = 12345
+    out = {}
+    for name, fn in (("remove_max", lambda a: vcgpu.remove_max_ub(a)), ("remove_edge", lambda a: vcgpu.remove_edge_ub(a, r))):
+        fn(g5)  # warm-up
+        t0 = time.perf_counter()
+        ubs, _, kms = fn(g5)
+        call_ms = 1e3 * (time.perf_counter() - t0)
+        _, _, bms = fn(arena)
+        out[name] = {"config5_bound": ubs[0], "config5_kernel_ms": kms, "config5_call_ms": call_ms,
+                     "batch_kernel_ms": bms}
+    cpu = {}
+    if os.path.exists(os.path.join(REPO, "oracle", "_ref", "libvcref.so")):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as O
+        for name, fn in (("remove_max", O.ref_remove_max_ub_forked), ("remove_edge", O.ref_remove_edge_ub_forked)):
+            t0 = time.perf_counter()
+            fn(g5)
+            cpu[name + "_config5_s"] = time.perf_counter() - t0
+    line = {"metric": "upper-bound heuristics time (config 5, Chung-Lu n=100000)",
+            "value": out["remove_edge"]["config5_call_ms"], "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": out["remove_edge"]["config5_call_ms"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "RemoveMax / RemoveEdge upper bounds: Chung-Lu n=100000 (gamma 2.1, avg degree 8, "
+                                   f"max degree 2000, seed 7) and {args.count} batched G(n,p) graphs", **out,
+                       "reference_cpu": cpu}}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
@@ -437,6 +475,8 @@ def main():
             reference_arm(args, world, rank)
         elif args.workload == "stream":
             stream_arm(args, world, rank)
+        elif args.workload == "ub":
+            ub_arm(args, world, rank)
         else:
             our_arm(args, world, rank, local, pg)
     finally:
