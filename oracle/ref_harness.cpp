@@ -15,7 +15,6 @@
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
-#include <cstdlib>
 #include "CSRGraphRep.h"
 #include "Sequential.h"
 #include "SequentialParameterized.h"
