@@ -39,7 +39,15 @@ typedef enum vc_instance {
     VC_PVC = 1  /* parameterized vertex cover, decision size <= k (`-i pvc -k K`) */
 } vc_instance;
 
-/* vc_request.flags */
+/* vc_request.flags.  Host-resident graphs are checked on the host (monotone
+ * offsets, ids < n, no self loop or duplicate, sorted symmetric rows) unless
+ * VC_FLAG_NO_VALIDATE.  Device-resident graphs (VC_FLAG_DEVICE_INPUT, and
+ * vc_solve_batch_device) cannot be read by the host: a kernel checks the layout
+ * the search relies on for memory safety -- row_ptr[0] = 0, row_ptr[n] = 2m as
+ * stated by the caller, monotone offsets, ids < n, no self loop -- and a graph
+ * that fails is reported VC_ERR_INVALID without being searched.  Sortedness,
+ * duplicates and symmetry of device-resident rows are trusted: a graph that
+ * breaks them gets a wrong answer, never an access outside its arrays. */
 #define VC_FLAG_DEVICE_INPUT 0x1u /* vc_csr / arena pointers are device pointers */
 #define VC_FLAG_NO_VALIDATE 0x2u  /* skip the host-side CSR checks */
 

@@ -506,11 +506,17 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
     const uint32_t *rp = P.row_ptr + d.row_off, *cl = P.col + d.col_off;
     for (uint32_t i = lane; i < Rows<NW>::kTri + (uint32_t)NW; i += 32) adj[i] = 0;
     __syncwarp();
+    // Entries that break the CSR layout (a row past row_ptr[n], an id out of
+    // range, a self loop) are skipped, so no read or write leaves its array;
+    // device-resident input is checked by k_check_csr before the search, which
+    // drops a graph it flags.
+    const uint32_t m2 = d.m2 != kNone ? min(__ldcg(&rp[d.n]), d.m2) : __ldcg(&rp[d.n]);
     for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
         uint32_t *row = adj + v * Rows<NW>::kStride;
-        const uint32_t e1 = __ldcg(&rp[v + 1]);
+        const uint32_t e1 = min(__ldcg(&rp[v + 1]), m2);
         for (uint32_t e = __ldcg(&rp[v]); e < e1; ++e) {
             const uint32_t u = __ldcg(&cl[e]);
+            if (u >= d.n || u == v) continue;
             row[u >> 5] |= 1u << (u & 31u);
         }
     }
@@ -751,8 +757,8 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
             c_state = G::bcast64(w);
         }
         ++ticks;
-        if (c_flags & (kFound | kBudget | kError)) {
-            if (lane == 0 && !(c_flags & (kFound | kBudget))) atomicOr(&st.flags, kCut);
+        if (c_flags & (kFound | kBudget | kError | kBadGraph)) {
+            if (lane == 0 && !(c_flags & (kFound | kBudget | kBadGraph))) atomicOr(&st.flags, kCut);
             s.fr_bot = s.fr_top = 0;
             s.pending = 0;
             if (lane < NW) s.marks()[lane] = 0;

@@ -19,6 +19,23 @@ namespace vch {
 constexpr uint32_t kWarpMaxNP = VC_WARP_MAX_NP;
 constexpr uint32_t kMaxVertices = 1u << 26;
 
+// Puts the calling thread's current device back when an entry point returns:
+// the library switches devices for its own work, never for its caller.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard()
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard &) = delete;
+    DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
@@ -38,6 +55,7 @@ struct Plan {
     uint32_t np = 0, su_bytes = 0, num_su = 0, stride = 0, cta_slots = 0;
     bool global_ws = false;
     bool dense = false;
+    bool lanes = false;  // one thread per search unit (vc_lanes.cuh)
 };
 
 // Per-device state: one stream, grow-only device and pinned buffers, a lock
@@ -54,6 +72,7 @@ struct Ctx {
     unsigned long long h_ctl[vcg::kCtlWords] = {};
     bool stats_on = false;
     bool force_sparse = false;
+    int lanes_mode = 0;  // graphs <= 255 vertices: 0 warp search units (default), 1 lane search units
     DevBuf stats;
     std::vector<unsigned long long> last_stats;
     uint32_t last_num_su = 0;
@@ -73,6 +92,7 @@ struct Job {
     unsigned long long t0 = 0;
     bool aborted = false;
     bool wide = false;  // every graph may take the 20-word dense kernel
+    bool dev_input = false;  // the graphs came from the caller's device memory: checked by k_check_csr
     Plan plan;
 };
 
@@ -94,6 +114,7 @@ struct PlanOpts {
     uint32_t warps = 0;        // warps per CTA with warp_gws, 0 = 8
     bool wide = false;         // graphs of 256..640 vertices may take the wide dense kernel
     bool warp_gws = false;     // warp units with global-memory workspaces
+    bool lanes = false;        // graphs <= 255 vertices take the lane kernel
 };
 
 Ctx *get_ctx(int dev, vc_status *err);

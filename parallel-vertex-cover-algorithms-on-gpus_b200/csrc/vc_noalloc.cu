@@ -28,6 +28,7 @@
 #include <mutex>
 
 #include "vc_dense.cuh"
+#include "vc_host.h"
 #include "vcgpu.h"
 
 using namespace vcg;
@@ -35,6 +36,9 @@ using namespace vcg;
 namespace vcn {
 
 constexpr uint32_t kNoAllocMaxVertices = 255;
+// A search unit gives a record to the ring only while more CTAs are idle than
+// records are queued, so at most one record per CTA is ever pending: the grid
+// is at most 4 CTAs per SM (1024 threads), 592 on a B200, well inside the ring.
 constexpr uint32_t kRingSlots = 4096;
 constexpr uint32_t kMaxStride = 12;  // 4 header words + 8 bitmap words
 constexpr size_t kScratchBytes = 256 * 1024;
@@ -104,7 +108,8 @@ __global__ void k_noalloc_finish(const Scratch *s, uint32_t ub, uint32_t *result
     if (cover && i < d.nw) cover[i] = has_cover ? s->cover[i] : 0u;
     if (i != 0) return;
     uint32_t status;
-    if (st.flags & kError) status = VC_ERR_INTERNAL;
+    if (st.flags & kBadGraph) status = VC_ERR_INVALID;
+    else if (st.flags & kError) status = VC_ERR_INTERNAL;
     else if (st.flags & kBudget) status = VC_BUDGET;
     else if ((st.flags & kCut) || !(st.flags & kDone)) status = s->ctl[kAbort] ? VC_TIMEOUT : VC_ERR_INTERNAL;
     else status = VC_OK;
@@ -197,6 +202,7 @@ using namespace vcn;
 // set = v in the cover).  Values have the meaning of vc_result's fields.
 extern "C" vc_status vc_solve_noalloc(const vc_csr *g, const vc_request *req, uint32_t *d_result, uint32_t *d_cover)
 {
+    vch::DeviceGuard dg;
     if (!g || !req || !d_result) return VC_ERR_INVALID;
     if (!(req->flags & VC_FLAG_DEVICE_INPUT)) return VC_ERR_INVALID;
     if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
@@ -226,11 +232,28 @@ extern "C" vc_status vc_solve_noalloc(const vc_csr *g, const vc_request *req, ui
     d.cover_off = 0;
     d.node_limit = req->node_limit;
     d.key = 0;
-    d.pad = 0;
+    d.m2 = 2ull * g->m < (uint64_t)kNone ? (uint32_t)(2ull * g->m) : kNone;
 
+    // Launches are checked through their own return codes, so an error the
+    // caller's earlier work left pending is neither reported nor cleared here.
     Scratch *s = su->scratch;
-    k_noalloc_reset<<<(kRingSlots + 255) / 256, 256, 0, stream>>>(s, d);
-    if (cudaGetLastError() != cudaSuccess) return VC_ERR_CUDA;
+    {
+        void *a[] = {&s, &d};
+        if (cudaLaunchKernel((const void *)k_noalloc_reset, dim3((kRingSlots + 255) / 256), dim3(256), a, 0, stream) !=
+            cudaSuccess)
+            return VC_ERR_CUDA;
+    }
+    {
+        // the caller's CSR is device memory: check its layout before the search
+        // reads it (a graph that fails is reported VC_ERR_INVALID)
+        const uint32_t *rp = g->row_ptr, *cl = g->col;
+        const InstDesc *di = &s->desc;
+        InstState *sti = &s->st;
+        uint32_t one = 1;
+        void *a[] = {&rp, &cl, &di, &sti, &one};
+        if (cudaLaunchKernel((const void *)k_check_csr<0>, dim3(1), dim3(256), a, 0, stream) != cudaSuccess)
+            return VC_ERR_CUDA;
+    }
 
     Params P;
     memset(&P, 0, sizeof(P));
@@ -258,7 +281,12 @@ extern "C" vc_status vc_solve_noalloc(const vc_csr *g, const vc_request *req, ui
                               : (idx == 1 ? (const void *)k_dense_noalloc<4, 256> : (const void *)k_dense_noalloc<8, 256>);
     if (cudaLaunchCooperativeKernel(fn, dim3(su->grid[idx]), dim3(256), args, su->smem[idx], stream) != cudaSuccess)
         return VC_ERR_CUDA;
-    k_noalloc_finish<<<1, 32, 0, stream>>>(s, ub, d_result, d_cover);
-    if (cudaGetLastError() != cudaSuccess) return VC_ERR_CUDA;
+    {
+        const Scratch *cs = s;
+        uint32_t ubv = ub;
+        void *a[] = {&cs, &ubv, &d_result, &d_cover};
+        if (cudaLaunchKernel((const void *)k_noalloc_finish, dim3(1), dim3(32), a, 0, stream) != cudaSuccess)
+            return VC_ERR_CUDA;
+    }
     return VC_OK;
 }

@@ -82,8 +82,35 @@ __device__ __forceinline__ InstDesc load_desc(const InstDesc *p)
     d.cover_off = __ldcg(&p->cover_off);
     d.node_limit = __ldcg(&p->node_limit);
     d.key = __ldcg(&p->key);
-    d.pad = 0;
+    d.m2 = __ldcg(&p->m2);
     return d;
+}
+
+// Device-resident graphs: one CTA per graph checks the CSR layout the kernels
+// rely on (row_ptr[0] = 0, row_ptr[n] = the 2m the caller stated, monotone
+// offsets, ids < n, no self loops) and flags a graph that breaks it, so the
+// search never reads or writes outside the caller's arrays.
+template <int Unused>
+__global__ void k_check_csr(const uint32_t *row_ptr, const uint32_t *col, const InstDesc *inst, InstState *st,
+                            uint32_t count)
+{
+    for (uint32_t gi = blockIdx.x; gi < count; gi += gridDim.x) {
+        const InstDesc d = inst[gi];
+        const uint32_t *rp = row_ptr + d.row_off, *cl = col + d.col_off;
+        const uint32_t m2 = rp[d.n];
+        bool bad = rp[0] != 0u || (d.m2 != kNone && m2 != d.m2);
+        if (!bad) {
+            for (uint32_t v = threadIdx.x; v < d.n; v += blockDim.x) {
+                const uint32_t e0 = rp[v], e1 = rp[v + 1];
+                if (e1 < e0 || e1 > m2) { bad = true; break; }
+                for (uint32_t e = e0; e < e1; ++e) {
+                    const uint32_t u = cl[e];
+                    if (u >= d.n || u == v) { bad = true; break; }
+                }
+            }
+        }
+        if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&st[gi].flags, kBadGraph);
+    }
 }
 
 // ---------------------------------------------------------------- groups
@@ -732,7 +759,7 @@ __device__ __forceinline__ bool start_record(S &s, const Params &P)
     uint32_t fl = 0;
     if (G::rank() == 0) fl = ld_relaxed_u32(&P.st[s.inst].flags);
     fl = G::bcast(fl);
-    if (fl & (kFound | kBudget | kError)) {
+    if (fl & (kFound | kBudget | kError | kBadGraph)) {
         finish_stint<G, S>(s, P);
         return false;
     }
@@ -937,8 +964,8 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
             c_state = G::bcast64(w);
         }
         ++ticks;
-        if (c_flags & (kFound | kBudget | kError)) {  // abandon this graph
-            if (G::rank() == 0 && !(c_flags & (kFound | kBudget))) atomicOr(&st.flags, kCut);
+        if (c_flags & (kFound | kBudget | kError | kBadGraph)) {  // abandon this graph
+            if (G::rank() == 0 && !(c_flags & (kFound | kBudget | kBadGraph))) atomicOr(&st.flags, kCut);
             s.fr_bot = s.fr_top = 0;
             have = false;
             continue;

@@ -213,6 +213,7 @@ uint32_t admit(SrvLane *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
         d.cover_off = slot * s->nw_max;
         d.node_limit = p.req.node_limit;
         d.key = (uint32_t)p.ticket;
+        d.m2 = kNone;  // host-validated graphs
         descs.push_back(d);
         HostResult *hr = reinterpret_cast<HostResult *>(s->h_res + (size_t)slot * s->res_words);
         hr->done = 0;  // the previous occupant's record
@@ -590,6 +591,7 @@ inline SrvLane *lane_of(vc_server *s, uint64_t ticket, uint64_t *lt)
 extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes, uint32_t max_requests,
                                      uint32_t max_vertices, vc_server **out)
 {
+    vch::DeviceGuard dg;
     if (!out) return VC_ERR_INVALID;
     *out = nullptr;
     vc_status err;
@@ -641,6 +643,7 @@ extern "C" vc_status vc_server_create(int32_t device, uint64_t mem_budget_bytes,
 
 extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_request *req, uint64_t *ticket)
 {
+    vch::DeviceGuard dg;
     if (!s || !g || !req || !ticket) return VC_ERR_INVALID;
     if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
     if (req->flags & VC_FLAG_DEVICE_INPUT) return VC_ERR_INVALID;  // the server copies from host memory
@@ -674,6 +677,7 @@ extern "C" vc_status vc_server_submit(vc_server *s, const vc_csr *g, const vc_re
 
 extern "C" vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *out)
 {
+    vch::DeviceGuard dg;
     if (!s || !out) return VC_ERR_INVALID;
     uint64_t lt = 0;
     SrvLane *l = lane_of(s, ticket, &lt);
@@ -703,6 +707,7 @@ extern "C" vc_status vc_server_poll(vc_server *s, uint64_t ticket, vc_result *ou
 
 extern "C" vc_status vc_server_completed(vc_server *s, uint64_t *tickets, uint32_t max_tickets, uint32_t *count)
 {
+    vch::DeviceGuard dg;
     if (!s || !count || (max_tickets && !tickets)) return VC_ERR_INVALID;
     uint32_t k = 0;
     for (uint32_t li = 0; li < s->lanes.size(); ++li) {
@@ -737,6 +742,7 @@ extern "C" vc_status vc_server_shape(vc_server *s, uint32_t *shape, uint32_t max
 
 extern "C" vc_status vc_server_destroy(vc_server *s)
 {
+    vch::DeviceGuard dg;
     if (!s) return VC_ERR_INVALID;
     // all lanes stop together: a lane's kernel can only finish once all its
     // CTAs have run, which may need another lane's kernel to leave its SMs

@@ -18,6 +18,7 @@
 
 #include "vc_search.cuh"
 #include "vc_dense.cuh"
+#include "vc_lanes.cuh"
 #include "vc_host.h"
 #include "vcgpu.h"
 
@@ -96,6 +97,25 @@ __global__ void __launch_bounds__(NT, DenseOcc<NW>::template min_ctas<NT>()) k_d
     for (uint32_t i = threadIdx.x; i < P.cta_slots; i += blockDim.x) cp.state[i] = 0;
     __syncthreads();
     su_main_dense<NW>(P, ws0 + (size_t)WarpG::su_local() * P.su_bytes, adj, cp);
+}
+
+// One thread per search unit (vc_lanes.cuh); NT lanes per CTA.
+#ifndef VC_LANE_THREADS
+#define VC_LANE_THREADS 128
+#endif
+template <int NW, unsigned NT>
+__global__ void __launch_bounds__(NT, 1) k_lanes(Params P)
+{
+    extern __shared__ __align__(16) uint32_t lsm[];
+    __shared__ uint32_t hdr[kLhWords];
+    const LaneLayout lo(P.np / 32u, NW, NT, P.cta_slots);
+    if (threadIdx.x < kLhWords) {
+        const uint32_t i = threadIdx.x;
+        hdr[i] = i == kLhIdle ? NT : ((i == kLhGraph || i == kLhKey) ? kNone : 0u);
+    }
+    for (uint32_t i = threadIdx.x; i < P.cta_slots; i += NT) lsm[lo.sstate + i] = 0;
+    __syncthreads();
+    lanes_main<NW, NT>(P, lsm, hdr);
 }
 
 __global__ void k_init_ring(unsigned long long *seq, uint32_t q)
@@ -178,6 +198,8 @@ Ctx *get_ctx(int dev, vc_status *err)
         c->sms = prop.multiProcessorCount;
         c->smem_optin = (int)prop.sharedMemPerBlockOptin;
         c->coop = prop.cooperativeLaunch;
+        // VC_LANES=1 selects lane search units for graphs of at most 255 vertices
+        if (const char *e = getenv("VC_LANES")) c->lanes_mode = atoi(e) ? 1 : 0;
         if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
             delete c;
@@ -261,9 +283,34 @@ static cudaError_t plan_dense(Ctx &c, Plan &pl)
     return cudaSuccess;
 }
 
+template <int NW>
+static cudaError_t plan_lanes(Ctx &c, Plan &pl, uint32_t nmax)
+{
+    constexpr unsigned NT = VC_LANE_THREADS;
+    const uint32_t nwc = std::max<uint32_t>(1, (nmax + 31) / 32);
+    pl.np = 32 * nwc;
+    pl.stride = (4 + NW + 3) / 4 * 4;
+    pl.cta_slots = kLanePoolSlots;
+    const LaneLayout lo(nwc, NW, NT, pl.cta_slots);
+    pl.su_bytes = 4u * (17u * nwc);  // degree bytes, trail bytes, flag words per lane
+    cudaError_t e = plan_variant_fn<NT>(c, pl, 4u * lo.words, k_lanes<NW, NT>);
+    if (e != cudaSuccess) return e;
+    pl.num_su = pl.grid * NT;
+    pl.global_ws = false;
+    pl.dense = true;
+    pl.lanes = true;
+    return cudaSuccess;
+}
+
 cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOpts &o)
 {
     pl.dense = false;
+    pl.lanes = false;
+    if (o.lanes && !c.force_sparse && nmax <= 255) {
+        if (nmax <= 64) return plan_lanes<2>(c, pl, nmax);
+        if (nmax <= 128) return plan_lanes<4>(c, pl, nmax);
+        return plan_lanes<8>(c, pl, nmax);
+    }
     const uint32_t smem_budget = o.smem_budget, warp_max_np = o.warp_max_np;
     // dense bitsets up to 255 vertices, and up to 640 when every degree fits a
     // byte (degrees are bytes; 0 = removed or isolated)
@@ -354,10 +401,16 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     Plan pl;
     PlanOpts po;
     po.wide = job.wide;
+    // Lane units (one thread per search unit, vc_lanes.cuh) are opt-in: they
+    // execute half the instructions per tree node of warp units but, at 12
+    // resident warps per SM, issue on a fifth of the cycles (ncu, batched
+    // workload) and reach a quarter of the warp units' node rate.
+    po.lanes = c.lanes_mode == 1;
     if (make_plan(c, np, nmax, pl, po) != cudaSuccess) return VC_ERR_CUDA;
     const uint32_t stride = pl.stride;
     uint32_t q = 1024;
-    while (q < 2 * pl.num_su) q <<= 1;
+    const uint32_t ring_units = pl.lanes ? pl.grid : pl.num_su;  // lane CTAs poll the ring as a whole
+    while (q < 2 * ring_units) q <<= 1;
     const size_t ring_cap_bytes = (size_t)512 << 20;
     while (q > 64 && (size_t)q * stride * 4 > ring_cap_bytes) q >>= 1;
 
@@ -379,6 +432,11 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     k_init_ring<<<(q + 255) / 256, 256, 0, stream>>>((unsigned long long *)c.seq.p, q);
     k_init_state<<<(count + 255) / 256, 256, 0, stream>>>((InstState *)c.st.p, (const InstDesc *)c.inst.p, count);
     g_launches += 2;
+    if (job.dev_input) {
+        k_check_csr<0><<<std::min<uint32_t>(count, 4096), 256, 0, stream>>>(job.d_rp, job.d_col, (const InstDesc *)c.inst.p,
+                                                                        (InstState *)c.st.p, count);
+        g_launches += 1;
+    }
 
     Params P;
     memset(&P, 0, sizeof(P));
@@ -443,7 +501,8 @@ vc_status fill_result(const Job &job, uint32_t i, uint32_t ub, vc_result *out)
     const InstDesc &d = job.desc[i];
     const InstState &s = job.st[i];
     vc_status st;
-    if (s.flags & kError) st = VC_ERR_INTERNAL;
+    if (s.flags & kBadGraph) st = VC_ERR_INVALID;
+    else if (s.flags & kError) st = VC_ERR_INTERNAL;
     else if (s.flags & kBudget) st = VC_BUDGET;
     else if ((s.flags & kCut) || !(s.flags & kDone)) st = job.aborted ? VC_TIMEOUT : VC_ERR_INTERNAL;
     else st = VC_OK;
@@ -496,20 +555,23 @@ extern "C" const char *vc_status_string(vc_status s)
 
 extern "C" uint64_t vc_kernel_launches(void) { return g_launches.load(); }
 
-// Diagnostics (not part of the reference surface): enable per-search-unit
-// counters on a device, and read the last launch's counters as rows of
+// Diagnostics (not part of the reference surface): enable (bit 0)
+// per-search-unit counters on a device, force the CSR kernel (bit 1) or lane
+// search units (bit 2) for graphs of at most 255 vertices, and read the last launch's counters as rows of
 // kStatWords u64 (nodes, passes, donations, failed donations, receives, roots,
 // busy cycles, idle cycles, polls, restored vertices, SM id).  Returns the
 // number of search units; copies at most max_rows rows.
 extern "C" uint32_t vc_debug_stats(int32_t device, int32_t enable, uint64_t *rows, uint32_t max_rows,
                                    uint32_t *launch_shape)
 {
+    vch::DeviceGuard dg;
     vc_status err;
     Ctx *c = get_ctx(device, &err);
     if (!c) return 0;
     std::lock_guard<std::mutex> lk(c->mu);
     if (enable >= 0) c->stats_on = (enable & 1) != 0;
     if (enable >= 0) c->force_sparse = (enable & 2) != 0;
+    if (enable >= 0) c->lanes_mode = (enable & 4) ? 1 : 0;
     uint32_t nsu = c->last_num_su;
     if (rows) {
         // rows exist only for a launch that ran with the counters on
@@ -536,6 +598,7 @@ static uint32_t init_best_for(const vc_request *r, uint32_t n)
 
 extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result *out)
 {
+    vch::DeviceGuard dg;
     auto t0 = std::chrono::steady_clock::now();
     if (!g || !req || !out) return VC_ERR_INVALID;
     if (req->instance != VC_MVC && req->instance != VC_PVC) return VC_ERR_INVALID;
@@ -588,10 +651,11 @@ extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result 
     d.cover_off = 0;
     d.node_limit = req->node_limit;
     d.key = 0;
-    d.pad = 0;
+    d.m2 = 2ull * g->m < (uint64_t)kNone ? (uint32_t)(2ull * g->m) : kNone;
     job.desc.push_back(d);
     job.time_limit_s = req->time_limit_s;
     job.wide = !dev_in && wide_ok(g->n, g->row_ptr);
+    job.dev_input = dev_in;
     vc_status s = run_job(*c, job, stream);
     if (s != VC_OK) { out->status = s; return s; }
     s = fill_result(job, 0, req->instance == VC_MVC ? req->ub : 0, out);
@@ -601,6 +665,7 @@ extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result 
 
 extern "C" vc_status vc_solve_batch(const vc_csr_arena *a, const vc_request *reqs, vc_result *out)
 {
+    vch::DeviceGuard dg;
     auto t0 = std::chrono::steady_clock::now();
     if (!a || !reqs || !out) return VC_ERR_INVALID;
     if (a->count == 0) return VC_OK;
@@ -691,6 +756,7 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         cj.d_rp = job.d_rp;
         cj.d_col = job.d_col;
         cj.wide = cl == 1;
+        cj.dev_input = d_rp != nullptr;
         cj.desc.resize(members.size());
         double tl = 0;
         for (size_t j = 0; j < members.size(); ++j) {
@@ -705,7 +771,7 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
             d.init_best = init_best_for(&reqs[i], d.n);
             d.node_limit = reqs[i].node_limit;
             d.key = (uint32_t)j;
-            d.pad = 0;
+            d.m2 = a->row_ptr[a->row_off[i] + d.n];
             tl = std::max(tl, reqs[i].time_limit_s);
         }
         cj.time_limit_s = tl;
@@ -744,6 +810,7 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
 extern "C" vc_status vc_solve_batch_device(const vc_csr_arena *a, const uint32_t *d_rp, const uint32_t *d_col,
                                            const vc_request *reqs, vc_result *out)
 {
+    vch::DeviceGuard dg;
     auto t0 = std::chrono::steady_clock::now();
     if (!a || !reqs || !out || !d_rp) return VC_ERR_INVALID;
     if (a->count == 0) return VC_OK;

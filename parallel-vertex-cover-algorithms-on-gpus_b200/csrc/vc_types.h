@@ -21,6 +21,7 @@ constexpr uint32_t kBudget = 2u;  // node limit reached
 constexpr uint32_t kDone = 4u;    // every token of the graph returned
 constexpr uint32_t kError = 8u;   // a bounded wait gave up
 constexpr uint32_t kCut = 16u;    // work was dropped at the launch's time limit
+constexpr uint32_t kBadGraph = 32u;  // device-resident CSR failed the kernel's staging checks
 
 // control words, each on its own 128-byte line (index in u64 units)
 enum : uint32_t {
@@ -51,7 +52,7 @@ struct InstDesc {
     uint32_t cover_off;        // word offset of this graph's cover bitmap
     uint64_t node_limit;       // 0 = none
     uint32_t key;              // unique per graph (batch index / server ticket)
-    uint32_t pad;
+    uint32_t m2;               // row_ptr[n] (2m) as the host knows it, kNone = unknown
 };
 
 struct InstState {

@@ -439,11 +439,13 @@ vc_status ub_run(const vc_csr_arena *a, uint32_t mode, uint32_t r, int32_t devic
 extern "C" vc_status vc_remove_max_ub(const vc_csr_arena *a, int32_t device, uint32_t *ub, uint8_t *cover,
                                      float *kernel_ms)
 {
+    vch::DeviceGuard dg;
     return ub_run(a, 0u, 0u, device, ub, cover, kernel_ms);
 }
 
 extern "C" vc_status vc_remove_edge_ub(const vc_csr_arena *a, uint32_t r, int32_t device, uint32_t *ub,
                                       uint8_t *cover, float *kernel_ms)
 {
+    vch::DeviceGuard dg;
     return ub_run(a, 1u, r, device, ub, cover, kernel_ms);
 }

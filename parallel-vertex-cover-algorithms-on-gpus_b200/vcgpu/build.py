@@ -4,11 +4,15 @@
   output       -- the reference-compatible command line (`./output <args>`)
 
 Both land in the package directory so they travel with the source tree.
-Rebuilds only when a source is newer than its product.
+Each product is rebuilt unless the SHA-256 of its compile command and of every
+source and header it depends on equals the one recorded beside it when it was
+built (`<product>.srchash`): a prebuilt file is reused only for exactly these
+sources, whatever the file times say.
 """
 from __future__ import annotations
 
 import glob
+import hashlib
 import os
 import shutil
 import subprocess
@@ -30,11 +34,26 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _stale(product: str, sources) -> bool:
-    if not os.path.exists(product):
+def _digest(cmd, sources) -> str:
+    """Independent of where the tree lives (paths are taken relative to it)."""
+    h = hashlib.sha256(" ".join(c.replace(REPO, ".") for c in cmd).encode())
+    for path in sorted(sources):
+        h.update(os.path.relpath(path, REPO).encode())
+        with open(path, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def _stale(product: str, digest: str) -> bool:
+    if not os.path.exists(product) or not os.path.exists(product + ".srchash"):
         return True
-    t = os.path.getmtime(product)
-    return any(os.path.getmtime(s) > t for s in sources)
+    with open(product + ".srchash") as f:
+        return f.read().strip() != digest
+
+
+def _record(product: str, digest: str) -> None:
+    with open(product + ".srchash", "w") as f:
+        f.write(digest + "\n")
 
 
 def lib_sources():
@@ -46,18 +65,23 @@ def build(force: bool = False, verbose: bool = False) -> None:
     deps = srcs + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
         [os.path.join(REPO, "include", "vcgpu.h")]
     nvcc = _nvcc()
-    if force or _stale(LIB, deps):
-        cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-shared", "-o", LIB] + srcs
+    cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-shared", "-o", LIB] + srcs
+    dig = _digest([os.path.basename(c) if c == nvcc else c for c in cmd], deps)
+    if force or _stale(LIB, dig):
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
+        _record(LIB, dig)
     main_src = os.path.join(CSRC, "main.cpp")
-    if os.path.exists(main_src) and (force or _stale(CLI, [main_src, LIB] + deps)):
+    if os.path.exists(main_src):
         cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-o", CLI, main_src, "-L" + PKG, "-lvcgpu",
                                             "-Xlinker", "-rpath,$ORIGIN"]
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        dig_cli = _digest([os.path.basename(c) if c == nvcc else c for c in cmd] + [dig], deps + [main_src])
+        if force or _stale(CLI, dig_cli):
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+            _record(CLI, dig_cli)
 
 
 if __name__ == "__main__":

@@ -348,3 +348,85 @@ def test_device_input_entry_points():
         torch.cuda.synchronize()
         r = vcgpu.solve_device(g.n, g.m, grp.data_ptr(), gcol.data_ptr(), "mvc", time_limit=TL)
         _check_mvc(g, r, opts[j])
+
+
+def _device_csr(torch, g, mutate=None):
+    rp = g.row_ptr.astype(np.int64).copy()
+    col = g.col.astype(np.int64).copy()
+    if mutate:
+        mutate(rp, col)
+    return (torch.from_numpy(rp.astype(np.int32)).cuda(), torch.from_numpy(col.astype(np.int32)).cuda())
+
+
+def test_device_input_layout_checked_on_the_device():
+    """Device-resident CSR cannot be validated on the host: a kernel checks the
+    layout the search relies on.  A neighbour id out of range, a self loop, a
+    decreasing row offset or a row_ptr[n] that disagrees with the stated m is
+    reported VC_ERR_INVALID -- for the dense kernel, the CSR kernel and in a batch
+    beside a good graph, which still gets its optimum -- and the device stays
+    usable."""
+    torch = pytest.importorskip("torch")
+    g = W.config1_graph()
+    opt = json.load(open(os.path.join(GOLDEN, "small.json")))["config1"]["opt"]
+
+    def bad_id(rp, col):
+        col[3] = g.n + 7
+
+    def self_loop(rp, col):
+        col[rp[5]] = 5
+
+    def decreasing(rp, col):
+        rp[10] = rp[12] + 1
+
+    def overlong(rp, col):
+        rp[-1] = rp[-1] + 4
+
+    for mutate in (bad_id, self_loop, decreasing, overlong):
+        d_rp, d_col = _device_csr(torch, g, mutate)
+        torch.cuda.synchronize()
+        r = vcgpu.solve_device(g.n, g.m, d_rp.data_ptr(), d_col.data_ptr(), "mvc", time_limit=TL)
+        assert r.status == vcgpu.VC_ERR_INVALID, (mutate.__name__, r)
+        vcgpu.debug_stats(2)  # the CSR kernel
+        try:
+            r = vcgpu.solve_device(g.n, g.m, d_rp.data_ptr(), d_col.data_ptr(), "mvc", time_limit=TL)
+        finally:
+            vcgpu.debug_stats(0)
+        assert r.status == vcgpu.VC_ERR_INVALID, (mutate.__name__, r)
+    # a batch on the device: graph 1 broken on the device only, graph 0 and 2 good
+    graphs = [g, g, g]
+    arena = W.pack(graphs)
+    rp = arena.row_ptr.astype(np.int64).copy()
+    col = arena.col.astype(np.int64).copy()
+    col[int(arena.col_off[1]) + 2] = g.n + 1
+    d_rp = torch.from_numpy(rp.astype(np.int32)).cuda()
+    d_col = torch.from_numpy(col.astype(np.int32)).cuda()
+    torch.cuda.synchronize()
+    st, sols = vcgpu.solve_batch(arena, "mvc", time_limit=TL, d_row_ptr=d_rp.data_ptr(), d_col=d_col.data_ptr())
+    assert sols[1].status == vcgpu.VC_ERR_INVALID
+    _check_mvc(g, sols[0], opt)
+    _check_mvc(g, sols[2], opt)
+    _check_mvc(g, vcgpu.solve(g, "mvc", time_limit=TL), opt)
+
+
+def test_lane_search_units_match_golden():
+    """The opt-in lane kernel (one thread per search unit) returns the oracle's
+    optimum with a verified cover on golden batch graphs, MVC and PVC, batched
+    and plain."""
+    recs = _golden_batch(300_000)[:160]
+    graphs = [W.batch_instance(r["i"]) for r in recs]
+    vcgpu.debug_stats(4)
+    try:
+        st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+        ks = [r["opt"] - (i % 2) for i, r in enumerate(recs[:40])]
+        stp, pv = vcgpu.solve_batch(W.pack(graphs[:40]), "pvc", ks=ks, time_limit=TL)
+        single = [vcgpu.solve(graphs[j], "mvc", time_limit=TL) for j in (0, 1, 2)]
+        shape = vcgpu.debug_stats()[1]
+    finally:
+        vcgpu.debug_stats(0)
+    assert int(shape[1]) != 256  # the lane kernel's CTA shape, not the dense kernel's
+    for g, r, rec in zip(graphs, sols, recs):
+        _check_mvc(g, r, rec["opt"])
+    for g, r, rec, k in zip(graphs, pv, recs, ks):
+        _check_pvc(g, r, k, 1 if rec["opt"] <= k else 0)
+    for j, r in zip((0, 1, 2), single):
+        _check_mvc(graphs[j], r, recs[j]["opt"])
