@@ -683,8 +683,8 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
             if (lane == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
             continue;
         }
-        if (lane == 0) __nanosleep(poller ? nap : 256);
-        nap = nap < 4096 ? nap * 2 : 4096;
+        if (lane == 0) __nanosleep(nap);
+        nap = nap < (poller ? 4096u : kIdleNapMax) ? nap * 2 : (poller ? 4096u : kIdleNapMax);
         __syncwarp();
     }
 }

@@ -714,8 +714,8 @@ __device__ void lanes_main(const Params &P, uint32_t *sm, uint32_t *hdr)
                 continue;
             }
             if (res == 0) {
-                if (lane == 0) __nanosleep(poller ? nap : 256);
-                nap = nap < 4096 ? nap * 2 : 4096;
+                if (lane == 0) __nanosleep(nap);
+                nap = nap < (poller ? 4096u : kIdleNapMax) ? nap * 2 : (poller ? 4096u : kIdleNapMax);
                 __syncwarp();
                 continue;
             }

@@ -113,6 +113,16 @@ __global__ void k_check_csr(const uint32_t *row_ptr, const uint32_t *col, const 
     }
 }
 
+// Idle search units that wait for work from their CTA (all but the CTA's one
+// ring poller) sleep with exponential back-off up to kIdleNapMax ns between
+// looks at the CTA pool.  Each look costs a few dozen instructions; dozens of
+// idle warps per SM looking every 256 ns took most of the SM's issue slots from
+// the busy warps when one graph had the whole GPU.
+#ifndef VC_IDLE_NAP_MAX
+#define VC_IDLE_NAP_MAX 16384u
+#endif
+constexpr uint32_t kIdleNapMax = VC_IDLE_NAP_MAX;
+
 // ---------------------------------------------------------------- groups
 struct WarpG {
     static constexpr unsigned kSize = 32;
@@ -901,8 +911,8 @@ __device__ bool acquire(S &s, const Params &P, CtaPool &cp, bool &cursor_open)
             if (G::rank() == 0) { __threadfence_block(); atomicAdd(&cp.hdr[kCpIdle], 1u); }
             continue;
         }
-        if (G::rank() == 0) __nanosleep(poller ? nap : 256);
-        nap = nap < 4096 ? nap * 2 : 4096;
+        if (G::rank() == 0) __nanosleep(nap);
+        nap = nap < (poller ? 4096u : kIdleNapMax) ? nap * 2 : (poller ? 4096u : kIdleNapMax);
         G::sync();
     }
 }
