@@ -18,6 +18,9 @@ from typing import Optional, Tuple
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# Where the reference tree is read from (its graph files, its runGraphs.py, its
+# sources for oracle/Makefile): $VC_REFERENCE_ROOT, by default /root/reference.
+REFERENCE_ROOT = os.environ.get("VC_REFERENCE_ROOT", "/root/reference")
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libvcref.so")
 

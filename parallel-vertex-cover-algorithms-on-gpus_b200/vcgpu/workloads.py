@@ -251,8 +251,11 @@ def pack(graphs: Sequence[Graph]) -> Arena:
 
 def read_reference_file(path: str, one_based: bool = True) -> Graph:
     """Reads the reference's text format: a header "n m", then m lines "u v"
-    (1-based ids, shifted down by one as src/auxFunctions.cpp:150-154 does)."""
-    with open(path, "r") as f:
+    (1-based ids, shifted down by one as src/auxFunctions.cpp:150-154 does; with
+    one_based=False the ids are taken as they are, the CLI's -z).  A path ending
+    in .gz is read through gzip."""
+    import gzip
+    with (gzip.open(path, "rt") if path.endswith(".gz") else open(path, "r")) as f:
         data = np.array(f.read().split(), dtype=np.int64)
     n, m = int(data[0]), int(data[1])
     e = data[2:2 + 2 * m].reshape(m, 2)

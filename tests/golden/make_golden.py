@@ -129,7 +129,7 @@ def files():
     running the reference's Sequential on each tractable 1-based file."""
     import oracle as O
     import re
-    ref_root = "/root/reference"
+    ref_root = O.REFERENCE_ROOT
     src = open(os.path.join(ref_root, "test", "runGraphs.py")).read()
     body = src[src.index("MVCS = {"):src.index("}", src.index("MVCS = {"))]
     golden = {k: int(v) for k, v in re.findall(r'"([^"]+)"\s*:\s*(\d+)', body)}

@@ -133,3 +133,25 @@ def test_cli_upper_bounds(tmp_path):
     assert edge >= O.mvc(g)[1]
     f = (tmp_path / "Results" / "Results.csv").read_text().strip().splitlines()[-1].split(",")
     assert f[14] == str(want) and f[16] == str(edge)
+
+
+@needs_cli
+@pytest.mark.gpu
+def test_cli_stack_only_version(tmp_path):
+    """-v stackonly (the reference's LocalStacks kernels, main.cu:306-308,340-342)
+    runs the same exact search: the same MVC size and PVC verdicts, with the
+    version field of the Results.csv row reading stackonly."""
+    g = W.config1_graph()
+    p = tmp_path / "g60.txt"
+    W.write_reference_file(g, str(p))
+    opt = O.mvc(g)[1]
+    r = run(["-v", "stackonly", "-d", "4", "-f", str(p), "-o", "s1"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert f"Size of minimum vertex cover: {opt}" in r.stdout
+    r = run(["-v", "stackonly", "-i", "pvc", "-k", str(opt - 1), "-f", str(p), "-o", "s2"], tmp_path)
+    assert r.returncode == 0 and f"Minimum is greater than K: {opt - 1}" in r.stdout
+    r = run(["-v", "stackonly", "-i", "pvc", "-k", str(opt), "-f", str(p), "-o", "s3"], tmp_path)
+    assert r.returncode == 0 and f"Minimum is less than or equal to K: {opt}" in r.stdout
+    rows = (tmp_path / "Results" / "Results.csv").read_text().strip().splitlines()
+    assert [row.split(",")[5] for row in rows] == ["stackonly"] * 3
+    assert rows[0].split(",")[18] == str(opt)

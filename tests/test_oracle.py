@@ -14,7 +14,7 @@ import oracle as O
 from vcgpu import workloads as W
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_ROOT = "/root/reference"
+REF_ROOT = O.REFERENCE_ROOT
 needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference CPU solver not built")
 
 
