@@ -77,6 +77,7 @@ def parse(argv=None):
     ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub", "profile"])
     ap.add_argument("--count", type=int, default=128)
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--case", default="batch", choices=["batch", "csr-batch", "powergrid"])
     ap.add_argument("--set", default="pinned", choices=["pinned", "full"])
     ap.add_argument("--time-limit", type=float, default=600.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -390,6 +391,7 @@ def served_leg(seconds, rate, node_limit=0):
     max_n = max(g.n for g, _ in pool)
     lat, bad, budget, done = [], 0, 0, 0
     lane_lat = {}
+    per_req = []  # (latency ms, tree nodes, lane, n)
     with vcgpu.Server(max_vertices=max_n, max_requests=4096, mem_budget=2 << 30) as srv:
         lanes = srv.shape()
         for g, opt in pool[:32]:  # warm-up: kernel launch, first-touch of buffers
@@ -409,6 +411,7 @@ def served_leg(seconds, rate, node_limit=0):
                 done += 1
                 lat.append(r.total_ms)
                 lane_lat.setdefault(vcgpu.Server.lane(tk), []).append(r.total_ms)
+                per_req.append((r.total_ms, r.tree_nodes, vcgpu.Server.lane(tk), g.n))
                 if r.status == vcgpu.VC_BUDGET:
                     budget += 1
                 elif r.status != vcgpu.VC_OK:
@@ -425,7 +428,17 @@ def served_leg(seconds, rate, node_limit=0):
         if li < len(lanes):
             lanes[li].update({"requests": len(x), "p50_latency_ms": float(np.percentile(x, 50)),
                               "p99_latency_ms": float(np.percentile(x, 99))})
-    return {"requests": len(reqs), "completed": done, "completed_per_s": done / wall, "wrong": bad,
+    # the tail: are the slowest 1% the requests with the most search work, or
+    # requests that waited behind others?
+    p99 = float(np.percentile(lat, 99))
+    tail = [x for x in per_req if x[0] >= p99]
+    nodes_all = np.asarray([x[1] for x in per_req], dtype=np.float64)
+    tail_info = {"requests": len(tail), "median_tree_nodes": float(np.median([x[1] for x in tail])) if tail else None,
+                 "median_tree_nodes_all": float(np.median(nodes_all)),
+                 "tail_share_of_top1pct_work": (sum(1 for x in tail if x[1] >= np.percentile(nodes_all, 99)) / len(tail))
+                 if tail else None,
+                 "median_n": float(np.median([x[3] for x in tail])) if tail else None}
+    return {"requests": len(reqs), "completed": done, "completed_per_s": done / wall, "wrong": bad, "tail": tail_info,
             "budget_exceeded": budget, "offered_per_s": rate, "seconds": seconds,
             "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
             "mean_latency_ms": float(lat.mean()), "pool": len(pool), "pool_coverage": len(pinned) / max(len(recs), 1),
@@ -692,11 +705,24 @@ def ub_arm(args, world, rank):
 
 
 def profile_arm(args):
-    """One small launch of the batched kernel without torch, for ncu: the first
-    --count graphs of the step's set, --reps times."""
+    """Small torch-free launches for ncu.  --case batch: the first --count graphs
+    of the step's set in one vc_solve_batch call (the dense kernel); csr-batch:
+    the same graphs with the CSR kernel forced; powergrid: the reference's
+    Power-Grid file (n = 4942, staged by `make -C oracle graphs`), one vc_solve
+    (the CSR kernel with CTA search units).  --reps times each."""
     import vcgpu
+    if args.case == "powergrid":
+        path = os.path.join(REPO, "oracle", "_ref", "graphs", "Power-Grid.txt.gz")
+        g = W.read_reference_file(path)
+        for it in range(args.reps):
+            r = vcgpu.solve(g, "mvc", time_limit=args.time_limit)
+            print(f"rep {it}: status {r.status} size {r.size} tree nodes {r.tree_nodes} kernel {r.kernel_ms:.1f} ms "
+                  f"{r.tree_nodes / max(r.kernel_ms, 1e-9) / 1e3:.1f} Mnodes/s", flush=True)
+        return
     idx = pinned_indices(args.set)[:args.count]
     arena = W.pack([W.batch_instance(i) for i in idx])
+    if args.case == "csr-batch":
+        vcgpu.debug_stats(2)
     for it in range(args.reps):
         st, sols = vcgpu.solve_batch(arena, "mvc", node_limit=args.node_limit, time_limit=args.time_limit)
         nodes = sum(s.tree_nodes for s in sols)

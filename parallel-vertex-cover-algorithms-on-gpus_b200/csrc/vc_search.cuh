@@ -68,6 +68,12 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p)
     return v;
 }
 
+// Graph rows and offsets.  A batch launch's arena is read-only while it runs
+// and goes through the non-coherent cache; a server launch's arena slots are
+// reused for new requests while the kernel runs, so it reads around L1
+// (ld.global.cg) and never sees a line of the slot's previous graph.
+__device__ __forceinline__ uint32_t gld(bool cg, const uint32_t *p) { return cg ? __ldcg(p) : __ldg(p); }
+
 // A graph descriptor read around L1 (server slots are rewritten during a launch).
 __device__ __forceinline__ InstDesc load_desc(const InstDesc *p)
 {
@@ -214,6 +220,7 @@ struct SU {
     uint32_t inst, n, nw, mode, k, cover_off;
     unsigned long long node_limit;
     uint32_t base_del;
+    bool cg;          // graph reads around L1 (server launches)
     uint32_t c_best;  // cached incumbent (refreshed every few nodes; stale values only weaken pruning)
     uint32_t fr_bot, fr_top;
     unsigned long long local_nodes;
@@ -240,12 +247,12 @@ __device__ __forceinline__ void su_bind(SU &s, uint8_t *ws, uint32_t np)
 
 __device__ __forceinline__ void mark(uint32_t *marks, uint32_t v) { atomicOr(&marks[v >> 5], 1u << (v & 31u)); }
 
-__device__ __forceinline__ bool row_contains(const uint32_t *rp, const uint32_t *cl, uint32_t row, uint32_t x)
+__device__ __forceinline__ bool row_contains(bool cg, const uint32_t *rp, const uint32_t *cl, uint32_t row, uint32_t x)
 {
-    uint32_t lo = __ldg(&rp[row]), hi = __ldg(&rp[row + 1]);
+    uint32_t lo = gld(cg, &rp[row]), hi = gld(cg, &rp[row + 1]);
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        uint32_t c = __ldg(&cl[mid]);
+        uint32_t c = gld(cg, &cl[mid]);
         if (c == x) return true;
         if (c < x) lo = mid + 1; else hi = mid;
     }
@@ -260,9 +267,9 @@ __device__ __forceinline__ void take_one(SU &s, uint32_t v)
     uint32_t idx = atomicAdd(&s.ctr[0], 1u);
     s.trail[idx] = v;
     volatile int32_t *dv = s.deg;
-    uint32_t e1 = __ldg(&s.rp[v + 1]);
-    for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
-        uint32_t u = __ldg(&s.cl[e]);
+    uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+    for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+        uint32_t u = gld(s.cg, &s.cl[e]);
         if (dv[u] >= 0) atomicSub(&s.deg[u], 1);
     }
 }
@@ -303,9 +310,9 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
     for (uint32_t i = G::rank(); i < nc; i += G::kSize) {
         const uint32_t v = s.cand[i];
         if (deg[v] == 1) {        // degree-one rule (helperFunctions.cuh:252-265)
-            uint32_t e1 = __ldg(&s.rp[v + 1]);
-            for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
-                uint32_t u = __ldg(&s.cl[e]);
+            uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+            for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+                uint32_t u = gld(s.cg, &s.cl[e]);
                 int32_t du = deg[u];
                 if (du > 0) {
                     if (du > 1 || u < v) { mark(s.marks, u); marked = true; }
@@ -315,16 +322,16 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
         } else {                  // degree-two triangle rule (helperFunctions.cuh:384-417)
             uint32_t n1 = kNone, n2 = kNone;
             bool keep = false;
-            uint32_t e1 = __ldg(&s.rp[v + 1]);
-            for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
-                uint32_t u = __ldg(&s.cl[e]);
+            uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+            for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+                uint32_t u = gld(s.cg, &s.cl[e]);
                 int32_t du = deg[u];
                 if (du > 0) {
                     if (du == 1 || (du == 2 && u < v)) { keep = true; break; }
                     if (n1 == kNone) n1 = u; else { n2 = u; break; }
                 }
             }
-            if (!keep && n2 != kNone && row_contains(s.rp, s.cl, n2, n1)) {
+            if (!keep && n2 != kNone && row_contains(s.cg, s.rp, s.cl, n2, n1)) {
                 mark(s.marks, n1);
                 mark(s.marks, n2);
                 marked = true;
@@ -369,9 +376,9 @@ __device__ __forceinline__ void take_vertex(SU &s, uint32_t v)
     ok = G::bcast(ok);
     if (ok) {
         volatile int32_t *dv = s.deg;
-        uint32_t e1 = __ldg(&s.rp[v + 1]);
-        for (uint32_t e = __ldg(&s.rp[v]) + G::rank(); e < e1; e += G::kSize) {
-            uint32_t u = __ldg(&s.cl[e]);
+        uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+        for (uint32_t e = gld(s.cg, &s.rp[v]) + G::rank(); e < e1; e += G::kSize) {
+            uint32_t u = gld(s.cg, &s.cl[e]);
             if (dv[u] >= 0) atomicSub(&s.deg[u], 1);
         }
     }
@@ -382,8 +389,8 @@ __device__ __forceinline__ void take_vertex(SU &s, uint32_t v)
 template <class G>
 __device__ __forceinline__ void take_neighbours(SU &s, uint32_t v)
 {
-    uint32_t e1 = __ldg(&s.rp[v + 1]);
-    for (uint32_t e = __ldg(&s.rp[v]) + G::rank(); e < e1; e += G::kSize) take_one(s, __ldg(&s.cl[e]));
+    uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+    for (uint32_t e = gld(s.cg, &s.rp[v]) + G::rank(); e < e1; e += G::kSize) take_one(s, gld(s.cg, &s.cl[e]));
     G::sync();
 }
 
@@ -400,9 +407,9 @@ __device__ __forceinline__ void restore_to(SU &s, uint32_t pos)
     for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {
         uint32_t v = s.trail[i];
         uint32_t c = 0;
-        uint32_t e1 = __ldg(&s.rp[v + 1]);
-        for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
-            uint32_t u = __ldg(&s.cl[e]);
+        uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+        for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+            uint32_t u = gld(s.cg, &s.cl[e]);
             int32_t d = dv[u];
             if (d == kRestoring) ++c;
             else if (d >= 0) { atomicAdd(&s.deg[u], 1); ++c; }
@@ -443,9 +450,9 @@ __device__ __forceinline__ void rebuild(SU &s)
         if (v >= s.n) { s.deg[v] = 0; continue; }
         if ((s.bits[v >> 5] >> (v & 31u)) & 1u) { s.deg[v] = kDead; continue; }
         uint32_t c = 0;
-        uint32_t e1 = __ldg(&s.rp[v + 1]);
-        for (uint32_t e = __ldg(&s.rp[v]); e < e1; ++e) {
-            uint32_t u = __ldg(&s.cl[e]);
+        uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+        for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+            uint32_t u = gld(s.cg, &s.cl[e]);
             c += ((s.bits[u >> 5] >> (u & 31u)) & 1u) ^ 1u;
         }
         s.deg[v] = (int32_t)c;
@@ -481,7 +488,7 @@ __device__ __forceinline__ void load_root(SU &s)
 {
     uint32_t pad_end = s.nw * 32;
     for (uint32_t v = G::rank(); v < pad_end; v += G::kSize)
-        s.deg[v] = v < s.n ? (int32_t)(__ldg(&s.rp[v + 1]) - __ldg(&s.rp[v])) : 0;
+        s.deg[v] = v < s.n ? (int32_t)(gld(s.cg, &s.rp[v + 1]) - gld(s.cg, &s.rp[v])) : 0;
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
     s.base_del = 0;
     if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; }
@@ -550,9 +557,9 @@ __device__ __forceinline__ void donation_bits(SU &s)
         atomicAnd(&s.bits[u >> 5], ~(1u << (u & 31u)));
     }
     G::sync();
-    uint32_t e1 = __ldg(&s.rp[v + 1]);
-    for (uint32_t e = __ldg(&s.rp[v]) + G::rank(); e < e1; e += G::kSize) {
-        uint32_t u = __ldg(&s.cl[e]);
+    uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+    for (uint32_t e = gld(s.cg, &s.rp[v]) + G::rank(); e < e1; e += G::kSize) {
+        uint32_t u = gld(s.cg, &s.cl[e]);
         atomicOr(&s.bits[u >> 5], 1u << (u & 31u));
     }
     G::sync();
@@ -922,6 +929,7 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
 {
     SU s;
     su_bind(s, ws, P.np);
+    s.cg = P.server != 0;
     s.inst = kNone;
     s.fr_bot = s.fr_top = 0;
     s.local_nodes = 0;

@@ -11,8 +11,13 @@
 //   * admits submitted requests into device slots while a slot and arena memory
 //     are free (admission by the request's device bytes: its CSR plus its cover
 //     bitmap; the search state itself lives in the kernel's fixed per-SU
-//     workspaces), copies the graph and its descriptor on a copy stream, and
-//     publishes the slot id on the device submission queue;
+//     workspaces, sized at creation for the largest request the lane takes),
+//     copies the graph and its descriptor on a copy stream, and publishes the
+//     slot id on the device submission queue.  Arena space is a first-fit free
+//     list: a finished request's block is reused for the next one while the
+//     kernel runs (the kernels read server graphs around L1, so no SM keeps a
+//     line of the block's previous graph), so a full arena only holds requests
+//     back until blocks free up -- the kernel never stops to empty it;
 //   * relaunches the kernel when it has exited (it exits after an idle period)
 //     and work is waiting;
 //   * collects results, which the SU that returns a request's last work token
@@ -26,6 +31,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -49,6 +55,7 @@ struct Pending {
 struct SlotInfo {
     uint64_t ticket = 0;
     uint32_t n = 0, ub = 0, mode = 0, init_best = 0;
+    uint64_t arena_off = 0, arena_len = 0;  // the request's arena block (bytes)
     std::chrono::steady_clock::time_point t_submit;
 };
 
@@ -85,7 +92,7 @@ struct SrvLane {
     std::unordered_map<uint64_t, Done> done;
     std::deque<uint64_t> ready;  // finished tickets not yet reported by vc_server_completed
     uint64_t next_ticket = 1;
-    uint64_t arena_bump = 0;
+    std::map<uint64_t, uint64_t> arena_free;  // free arena blocks: byte offset -> length
     uint64_t sub_tail = 0;
     bool running = false;
     bool resident = false;  // launched at creation and kept running (no idle exit)
@@ -176,6 +183,40 @@ bool wait_resident(SrvLane *s)
     return false;
 }
 
+// First-fit block of `bytes` (a multiple of 256) from the lane's arena; false
+// if no free block is large enough.
+bool arena_alloc(SrvLane *s, uint64_t bytes, uint64_t &off)
+{
+    for (auto it = s->arena_free.begin(); it != s->arena_free.end(); ++it) {
+        if (it->second < bytes) continue;
+        off = it->first;
+        const uint64_t rest = it->second - bytes;
+        s->arena_free.erase(it);
+        if (rest) s->arena_free.emplace(off + bytes, rest);
+        return true;
+    }
+    return false;
+}
+
+// Returns a block to the free list, merged with free neighbours.
+void arena_release(SrvLane *s, uint64_t off, uint64_t len)
+{
+    if (!len) return;
+    auto next = s->arena_free.lower_bound(off);
+    if (next != s->arena_free.end() && next->first == off + len) {
+        len += next->second;
+        next = s->arena_free.erase(next);
+    }
+    if (next != s->arena_free.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+            prev->second += len;
+            return;
+        }
+    }
+    s->arena_free.emplace(off, len);
+}
+
 // Admits pending requests into free slots (called by the loop, lock held):
 // copies their graphs and descriptors, then publishes their slot ids on the
 // submission queue with one synchronisation.  Returns the number admitted.
@@ -195,11 +236,11 @@ uint32_t admit(SrvLane *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
             s->pending.pop_front();
             continue;
         }
-        if (s->arena_bump + bytes > s->arena_cap) { arena_full = true; break; }
+        uint64_t boff = 0;
+        if (!arena_alloc(s, bytes, boff)) { arena_full = true; break; }
         const uint32_t slot = s->free_slots.back();
         s->free_slots.pop_back();
-        const uint64_t off = s->arena_bump / 4;
-        s->arena_bump += bytes;
+        const uint64_t off = boff / 4;
         InstDesc d;
         memset(&d, 0, sizeof(d));
         d.n = p.n;
@@ -224,6 +265,8 @@ uint32_t admit(SrvLane *s, std::unique_lock<std::mutex> &lk, bool &arena_full)
         si.mode = d.mode;
         si.init_best = d.init_best;
         si.t_submit = p.t_submit;
+        si.arena_off = boff;
+        si.arena_len = bytes;
         s->inflight.emplace(p.ticket, slot);
         published.push_back(slot);
         batch.push_back(std::move(p));
@@ -292,6 +335,8 @@ uint32_t collect(SrvLane *s)
         const uint32_t slot = s->inflight[t];
         s->inflight.erase(t);
         s->free_slots.push_back(slot);
+        arena_release(s, s->info[slot].arena_off, s->info[slot].arena_len);
+        s->info[slot].arena_len = 0;
         ++got;
     }
     return got;
@@ -306,6 +351,8 @@ void fail_inflight(SrvLane *s, vc_status st)
         s->done.emplace(kv.first, std::move(d));
         s->ready.push_back(kv.first);
         s->free_slots.push_back(kv.second);
+        arena_release(s, s->info[kv.second].arena_off, s->info[kv.second].arena_len);
+        s->info[kv.second].arena_len = 0;
     }
     s->inflight.clear();
 }
@@ -340,11 +387,6 @@ void request_loop(SrvLane *s)
             progress = true;
         }
         if (!s->stop) {
-            // The arena is a bump allocator whose addresses are never reused
-            // while one kernel launch runs (the search kernels read graphs
-            // through the non-coherent cache).  When it is full, in-flight work
-            // drains, the kernel is asked to stop, and the arena restarts empty.
-            if (!s->running && s->inflight.empty()) s->arena_bump = 0;
             // a resident kernel is restarted well before its 600 s limit: it
             // drains (no admissions) and exits, and the loop relaunches it
             if (s->resident && s->running && !s->draining &&
@@ -355,14 +397,8 @@ void request_loop(SrvLane *s)
                                 s->cstream);
                 cudaStreamSynchronize(s->cstream);
             }
-            bool arena_full = false;
+            bool arena_full = false;  // requests wait for blocks to free up
             if (!s->draining && admit(s, lk, arena_full)) progress = true;
-            if (arena_full && s->inflight.empty() && s->running) {
-                unsigned long long one = 1;
-                cudaMemcpyAsync((unsigned long long *)s->ctl.p + kShutdown, &one, sizeof(one), cudaMemcpyHostToDevice,
-                                s->cstream);
-                cudaStreamSynchronize(s->cstream);
-            }
             if ((!s->inflight.empty() || s->resident) && !s->running) {
                 vc_status st = launch_kernel(s);
                 if (st != VC_OK) s->fatal = st;
@@ -438,6 +474,8 @@ vc_status lane_create(Ctx *c, uint64_t budget, uint32_t slots, uint32_t max_n, c
     s->res_words = (uint32_t)(sizeof(HostResult) / 4) + s->nw_max;
     s->res_words = (s->res_words + 3) / 4 * 4;
     s->arena_cap = budget;
+    s->arena_free.clear();
+    s->arena_free.emplace(0, budget);
     bool ok = cudaStreamCreateWithFlags(&s->kstream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && !s->desc.ensure(sizeof(InstDesc) * s->slots) && !s->st.ensure(sizeof(InstState) * s->slots) &&

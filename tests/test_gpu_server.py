@@ -161,3 +161,22 @@ def test_server_lanes_small_and_large():
         _check(g, r, "mvc", 0, opt)
     for (g, opt), r in zip(items[::3], res[len(items):]):
         _check(g, r, "pvc", opt - 1, opt)
+
+
+def test_server_reuses_arena_blocks_while_running():
+    """An arena that holds only a handful of graphs at a time serves a stream of
+    many more: finished requests' blocks are reused while the lane's kernel keeps
+    running (no stop-and-drain), and every answer is still exact."""
+    recs = sorted((json.loads(l) for l in open(os.path.join(GOLDEN, "batch_seed0.jsonl")) if l.strip()),
+                  key=lambda r: r["i"])
+    easy = [r for r in recs if r["status"] == "ok" and r["nodes"] <= 20_000][:240]
+    graphs = [(W.batch_instance(r["i"]), r["opt"]) for r in easy]
+    biggest = max(((g.n + 1) + 2 * g.m) * 4 for g, _ in graphs)
+    # one lane (max_vertices <= 255); its arena is the whole budget
+    with vcgpu.Server(max_vertices=255, max_requests=64, mem_budget=6 * ((biggest + 255) // 256 * 256)) as srv:
+        tickets = []
+        for g, opt in graphs:
+            tickets.append((srv.submit(g, "mvc"), g, opt))
+        for tk, g, opt in tickets:
+            r = srv.wait(tk, timeout=120.0)
+            _check(g, r, "mvc", 0, opt)
