@@ -49,6 +49,30 @@ struct PinBuf {
     cudaError_t ensure(size_t bytes);
 };
 
+// A launch-shape choice for one size class of graphs, set by vc_autotune (or
+// vc_set_tuning); `set` = 0 keeps the built-in rules.
+struct Tune {
+    uint32_t set = 0;
+    uint32_t cta_units = 0;   // CSR classes: 1 = one 512-thread CTA per search unit, 0 = warp units
+    uint32_t warps = 8;       // warps (search units) per CTA: 2, 4 or 8
+    uint32_t pool = 2;        // CTA pool slots (donated subtrees) per warp: 1, 2 or 4
+    uint32_t ring_slack = 0;  // global-ring donations only while idle CTAs exceed queued records by more
+    float nodes_per_s = 0;    // what the calibration measured with this choice
+};
+
+// Size classes of the tuner: dense bitsets of 2, 4 and 8 words (n <= 64, 128,
+// 255), the wide dense kernel (n <= 640, degrees <= 254), CSR up to 1024
+// vertices, CSR above.
+constexpr int kTuneClasses = 6;
+inline int tune_class(uint32_t nmax, bool wide)
+{
+    if (nmax <= 64) return 0;
+    if (nmax <= 128) return 1;
+    if (nmax <= 255) return 2;
+    if (wide && nmax <= 640) return 3;
+    return nmax <= 1024 ? 4 : 5;
+}
+
 struct Plan {
     const void *fn = nullptr;
     uint32_t block = 0, grid = 0, smem = 0;
@@ -72,6 +96,7 @@ struct Ctx {
     unsigned long long h_ctl[vcg::kCtlWords] = {};
     bool stats_on = false;
     bool force_sparse = false;
+    Tune tune[kTuneClasses];
     int lanes_mode = 0;  // graphs <= 255 vertices: 0 warp search units (default), 1 lane search units
     DevBuf stats;
     std::vector<unsigned long long> last_stats;
@@ -93,6 +118,7 @@ struct Job {
     bool aborted = false;
     bool wide = false;  // every graph may take the 20-word dense kernel
     bool dev_input = false;  // the graphs came from the caller's device memory: checked by k_check_csr
+    const Tune *tune = nullptr;  // a shape to try instead of the context's table (the tuner's candidates)
     Plan plan;
 };
 
@@ -115,6 +141,7 @@ struct PlanOpts {
     bool wide = false;         // graphs of 256..640 vertices may take the wide dense kernel
     bool warp_gws = false;     // warp units with global-memory workspaces
     bool lanes = false;        // graphs <= 255 vertices take the lane kernel
+    const Tune *tune = nullptr; // the size class's tuned shape, if any
 };
 
 Ctx *get_ctx(int dev, vc_status *err);

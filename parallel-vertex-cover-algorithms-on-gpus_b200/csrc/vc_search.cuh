@@ -1040,7 +1040,7 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
         if (G::rank() == 0) {
             uint32_t li = vld(&cp.hdr[kCpIdle]), lc = vld(&cp.hdr[kCpCount]);
             if (li > lc) want = 1;
-            else if ((uint32_t)c_state > (uint32_t)(c_state >> 32)) want = 2;
+            else if ((uint32_t)c_state > (uint32_t)(c_state >> 32) + P.ring_slack) want = 2;
         }
         want = G::bcast(want);
         if (want == 1) donate_local<G, SU>(s, P, cp);

@@ -258,16 +258,17 @@ static cudaError_t plan_variant_fn(Ctx &c, Plan &pl, uint32_t smem_per_block, F 
 // shared memory while it fits, else in a global workspace.
 
 template <int NW>
-static cudaError_t plan_dense(Ctx &c, Plan &pl)
+static cudaError_t plan_dense(Ctx &c, Plan &pl, const Tune *t)
 {
     pl.np = 32 * NW;
     pl.su_bytes = dense_workspace_bytes(NW);
     pl.stride = (4 + NW + 3) / 4 * 4;
     const uint32_t budget = (uint32_t)c.smem_optin - 1024;
-    uint32_t warps = VC_DENSE_WARPS;  // search units sharing one staged graph
-    while (warps > 1 && dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget)
+    uint32_t warps = (t && t->set) ? t->warps : VC_DENSE_WARPS;  // search units sharing one staged graph
+    const uint32_t per_warp = (t && t->set) ? t->pool : 2;
+    while (warps > 1 && dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(per_warp * warps, pl.stride) > budget)
         warps >>= 1;
-    pl.cta_slots = warps > 1 ? 2 * warps : 0;
+    pl.cta_slots = warps > 1 ? per_warp * warps : 0;
     uint32_t smem = dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(pl.cta_slots, pl.stride);
     cudaError_t e;
     switch (warps) {
@@ -314,21 +315,28 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
     const uint32_t smem_budget = o.smem_budget, warp_max_np = o.warp_max_np;
     // dense bitsets up to 255 vertices, and up to 640 when every degree fits a
     // byte (degrees are bytes; 0 = removed or isolated)
-    if (nmax <= 64 && !c.force_sparse) return plan_dense<2>(c, pl);
-    if (nmax <= 128 && !c.force_sparse) return plan_dense<4>(c, pl);
-    if (nmax <= 255 && !c.force_sparse) return plan_dense<8>(c, pl);
-    if (nmax <= kWideMaxN && o.wide && !c.force_sparse) return plan_dense<20>(c, pl);
+    if (nmax <= 64 && !c.force_sparse) return plan_dense<2>(c, pl, o.tune);
+    if (nmax <= 128 && !c.force_sparse) return plan_dense<4>(c, pl, o.tune);
+    if (nmax <= 255 && !c.force_sparse) return plan_dense<8>(c, pl, o.tune);
+    if (nmax <= kWideMaxN && o.wide && !c.force_sparse) return plan_dense<20>(c, pl, o.tune);
+    const Tune *t = (o.tune && o.tune->set && !c.force_sparse) ? o.tune : nullptr;
     pl.np = np;
     pl.su_bytes = su_workspace_bytes(np);
     pl.stride = (4 + np / 32 + 3) / 4 * 4;
     const uint32_t static_smem = 1024;  // reductions / broadcasts / CTA pool header
     uint32_t budget = (uint32_t)c.smem_optin - static_smem;
     if (smem_budget) budget = std::min(budget, smem_budget > static_smem ? smem_budget - static_smem : 0u);
-    if (np <= (warp_max_np ? warp_max_np : kWarpMaxNP) && o.warp_gws) {
+    // a tuned choice: warp units (in shared memory where their workspaces fit,
+    // else in global memory) or CTA units
+    const bool tuned_warps = t && !t->cta_units;
+    const bool tuned_cta = t && t->cta_units;
+    const uint32_t per_warp = t ? t->pool : 2;
+    const bool warp_gws = o.warp_gws || (tuned_warps && np > kWarpMaxNP);
+    if (!tuned_cta && np <= (warp_max_np ? warp_max_np : (tuned_warps ? (1u << 16) : kWarpMaxNP)) && warp_gws) {
         // warp units with their workspaces in global memory: the CTA holds
         // only its pool
-        uint32_t warps = o.warps ? o.warps : 8;
-        pl.cta_slots = warps > 1 ? 2 * warps : 0;
+        uint32_t warps = t ? t->warps : (o.warps ? o.warps : 8);
+        pl.cta_slots = warps > 1 ? per_warp * warps : 0;
         const uint32_t smem = cta_pool_bytes(pl.cta_slots, pl.stride);
         cudaError_t e;
         switch (warps) {
@@ -342,11 +350,11 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
         pl.global_ws = true;
         return cudaSuccess;
     }
-    if (np <= (warp_max_np ? warp_max_np : kWarpMaxNP)) {
-        uint32_t warps = 8;
-        while (warps > 1 && warps * pl.su_bytes + cta_pool_bytes(2 * warps, pl.stride) > budget) warps >>= 1;
-        if (warps * pl.su_bytes + cta_pool_bytes(warps > 1 ? 2 * warps : 0, pl.stride) <= budget) {
-            pl.cta_slots = warps > 1 ? 2 * warps : 0;
+    if (!tuned_cta && np <= (warp_max_np ? warp_max_np : kWarpMaxNP)) {
+        uint32_t warps = t ? t->warps : 8;
+        while (warps > 1 && warps * pl.su_bytes + cta_pool_bytes(per_warp * warps, pl.stride) > budget) warps >>= 1;
+        if (warps * pl.su_bytes + cta_pool_bytes(warps > 1 ? per_warp * warps : 0, pl.stride) <= budget) {
+            pl.cta_slots = warps > 1 ? per_warp * warps : 0;
             uint32_t smem = warps * pl.su_bytes + cta_pool_bytes(pl.cta_slots, pl.stride);
             cudaError_t e;
             switch (warps) {
@@ -406,6 +414,8 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     // resident warps per SM, issue on a fifth of the cycles (ncu, batched
     // workload) and reach a quarter of the warp units' node rate.
     po.lanes = c.lanes_mode == 1;
+    const Tune *tn = job.tune ? job.tune : &c.tune[tune_class(nmax, job.wide)];
+    po.tune = tn->set ? tn : nullptr;
     if (make_plan(c, np, nmax, pl, po) != cudaSuccess) return VC_ERR_CUDA;
     const uint32_t stride = pl.stride;
     uint32_t q = 1024;
@@ -464,6 +474,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     }
     double tl = job.time_limit_s > 0 ? job.time_limit_s : 300.0;
     P.time_limit_ns = (unsigned long long)(tl * 1e9);
+    P.ring_slack = po.tune ? po.tune->ring_slack : 0u;
 
     void *args[] = {&P};
     cudaEventRecord(c.ev0, stream);

@@ -85,6 +85,7 @@ struct Params {
     uint8_t *gws;         // global workspace (CTA SUs on large graphs), else null
     unsigned long long *stats;    // per-SU counters (kStatWords each), null = off
     unsigned long long time_limit_ns;
+    uint32_t ring_slack;  // give work to the global ring only while idle CTAs exceed queued records by more than this
     // server mode (persistent kernel fed by the host)
     uint32_t server;
     uint32_t subq_mask;

@@ -286,6 +286,39 @@ def kernel_launches() -> int:
     return int(lib().vc_kernel_launches())
 
 
+TUNE_CLASSES = ["dense n<=64", "dense n<=128", "dense n<=255", "wide dense n<=640", "csr n<=1024", "csr n>1024"]
+
+
+def _unpack_tuning(buf: np.ndarray) -> List[dict]:
+    out = []
+    for i, name in enumerate(TUNE_CLASSES):
+        w = buf[6 * i:6 * i + 6]
+        out.append({"class": name, "set": int(w[0]), "units": "cta" if w[1] else "warp", "warps": int(w[2]),
+                    "pool_per_warp": int(w[3]), "ring_slack": int(w[4]),
+                    "nodes_per_s": float(np.frombuffer(np.uint32(w[5]).tobytes(), dtype=np.float32)[0])})
+    return out
+
+
+def autotune(slice_s: float = 0.0, device: int = -1):
+    """vc_autotune: measure launch shapes per size class on the device and install
+    the fastest.  Returns (status, table words, readable table)."""
+    buf = np.zeros(36, dtype=np.uint32)
+    L = lib()
+    L.vc_autotune.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_uint32]
+    L.vc_autotune.restype = ctypes.c_int
+    st = L.vc_autotune(device, slice_s, buf.ctypes.data, 36)
+    return st, buf, _unpack_tuning(buf)
+
+
+def set_tuning(table, device: int = -1) -> int:
+    """vc_set_tuning: install a table of words from autotune (zeros = built-in rules)."""
+    buf = np.ascontiguousarray(np.asarray(table, dtype=np.uint32))
+    L = lib()
+    L.vc_set_tuning.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint32]
+    L.vc_set_tuning.restype = ctypes.c_int
+    return L.vc_set_tuning(device, buf.ctypes.data, int(buf.size))
+
+
 class Server:
     """A continuous-batching server (vc_server_*): requests are admitted into a
     persistent kernel while others run."""
