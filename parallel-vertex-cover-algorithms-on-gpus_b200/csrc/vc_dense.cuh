@@ -602,17 +602,26 @@ __device__ bool acquire_cta(DSU<NW> &s, const Params &P, CtaPool &cp, uint32_t *
                         cp.hdr[kCpCursorClosed] = 1u;
                     }
                 }
-                if (res == 0 && (P.server || vld(&cp.hdr[kCpCursorClosed]))) {
+                // one graph in the launch (a plain solve): every record is for the
+                // graph this CTA already staged, so idle warps of a busy CTA may
+                // take records from the ring too
+                const bool single = P.count == 1 && !P.server;
+                if (res == 0 && (P.server || single || vld(&cp.hdr[kCpCursorClosed]))) {
                     unsigned long long stw = ld_relaxed_u64(&P.ctl[kState]);
                     if (!vld(&cp.hdr[kCpRegistered]) && cta_idle) {
                         stw = atomicAdd(&P.ctl[kState], 1ull) + 1ull;
                         cp.hdr[kCpRegistered] = 1u;
                     }
                     const bool reg = vld(&cp.hdr[kCpRegistered]) != 0;
+                    const bool staged = vld(&cp.hdr[kCpStaged]) != kNone;
                     // a registered CTA is fully idle, so the poller may switch graphs
-                    if (reg && (stw >> 32) > 0 && ring_claim_deq(P, qpos)) {
-                        atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle CTAs-1
-                        cp.hdr[kCpRegistered] = 0u;
+                    if ((reg || (single && staged)) && (stw >> 32) > 0 && ring_claim_deq(P, qpos)) {
+                        if (reg) {
+                            atomicAdd(&P.ctl[kState], 0xfffffffeffffffffull);  // pending-1, idle CTAs-1
+                            cp.hdr[kCpRegistered] = 0u;
+                        } else {
+                            atomicAdd(&P.ctl[kState], 0xffffffff00000000ull);  // pending-1
+                        }
                         atomicSub(&cp.hdr[kCpIdle], 1u);
                         res = 2;
                     } else if (reg && (uint32_t)stw == gridDim.x && (stw >> 32) == 0 &&
@@ -812,8 +821,14 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
         uint32_t want = 0;
         if (lane == 0) {
             uint32_t li = vld(&cp.hdr[kCpIdle]), lc = vld(&cp.hdr[kCpCount]);
-            if (li > lc) want = 1;
-            else if ((uint32_t)c_state > (uint32_t)(c_state >> 32) + P.ring_slack) want = 2;
+            const bool local_need = li > lc;
+            const bool ring_need = (long long)(uint32_t)c_state - (long long)(c_state >> 32) > (long long)P.ring_bias;
+            // both a sibling warp and another CTA wait: the policy decides (local
+            // first, ring first, or alternating)
+            if (local_need && ring_need)
+                want = (P.ring_first == 1 || (P.ring_first == 2 && (s.stat.donations & 1ull))) ? 2 : 1;
+            else if (local_need) want = 1;
+            else if (ring_need) want = 2;
         }
         want = G::bcast(want);
         if (want == 1) donate_local<G, S>(s, P, cp);

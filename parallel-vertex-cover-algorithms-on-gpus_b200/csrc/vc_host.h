@@ -56,7 +56,7 @@ struct Tune {
     uint32_t cta_units = 0;   // CSR classes: 1 = one 512-thread CTA per search unit, 0 = warp units
     uint32_t warps = 8;       // warps (search units) per CTA: 2, 4 or 8
     uint32_t pool = 2;        // CTA pool slots (donated subtrees) per warp: 1, 2 or 4
-    uint32_t ring_slack = 0;  // global-ring donations only while idle CTAs exceed queued records by more
+    int32_t ring_bias = 0;    // global-ring donations while idle CTAs minus queued records exceed this
     float nodes_per_s = 0;    // what the calibration measured with this choice
 };
 

@@ -902,7 +902,7 @@ __device__ void lanes_main(const Params &P, uint32_t *sm, uint32_t *hdr)
             if (lane == 0) {
                 const uint32_t li = vld(&hdr[kLhIdle]), lc = vld(&hdr[kLhCount]);
                 if (li > lc) want = min(li - lc, (uint32_t)__popc(cand));
-                else if ((uint32_t)stw > (uint32_t)(stw >> 32) + P.ring_slack) ring = 1;
+                else if ((long long)(uint32_t)stw - (long long)(stw >> 32) > (long long)P.ring_bias) ring = 1;
             }
             want = __shfl_sync(FULL, want, 0);
             ring = __shfl_sync(FULL, ring, 0);

@@ -1039,8 +1039,14 @@ __device__ void su_main(const Params &P, uint8_t *ws, CtaPool &cp)
         uint32_t want = 0;
         if (G::rank() == 0) {
             uint32_t li = vld(&cp.hdr[kCpIdle]), lc = vld(&cp.hdr[kCpCount]);
-            if (li > lc) want = 1;
-            else if ((uint32_t)c_state > (uint32_t)(c_state >> 32) + P.ring_slack) want = 2;
+            const bool local_need = li > lc;
+            const bool ring_need = (long long)(uint32_t)c_state - (long long)(c_state >> 32) > (long long)P.ring_bias;
+            // both a sibling warp and another CTA wait: the policy decides (local
+            // first, ring first, or alternating)
+            if (local_need && ring_need)
+                want = (P.ring_first == 1 || (P.ring_first == 2 && (s.stat.donations & 1ull))) ? 2 : 1;
+            else if (local_need) want = 1;
+            else if (ring_need) want = 2;
         }
         want = G::bcast(want);
         if (want == 1) donate_local<G, SU>(s, P, cp);

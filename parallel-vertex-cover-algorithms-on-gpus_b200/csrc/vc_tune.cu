@@ -12,8 +12,9 @@
 //     and one CTA pool,
 //   * CTA pool slots per warp (1, 2, 4) -- the depth of the shared-memory stack
 //     of donated subtrees,
-//   * the ring threshold: work goes to the global ring only while idle CTAs
-//     exceed the records already queued by more than 0, 4 or 32,
+//   * the ring threshold: work goes to the global ring while idle CTAs minus
+//     the records already queued exceed -64, -16, 0, 4 or 32 (a negative
+//     threshold keeps a surplus of records queued for CTAs that go idle),
 // on seeded calibration graphs of the class (G(n, p) of the batched family's
 // degrees, sizes spread over the class), each candidate timed for a fixed time
 // slice, and installs the winner in the device's table; later solves of that
@@ -146,7 +147,7 @@ void pack(const Tune *t, uint32_t *w)
         o[1] = t[i].cta_units;
         o[2] = t[i].warps;
         o[3] = t[i].pool;
-        o[4] = t[i].ring_slack;
+        memcpy(&o[4], &t[i].ring_bias, 4);
         memcpy(&o[5], &t[i].nodes_per_s, 4);
     }
 }
@@ -154,7 +155,7 @@ void pack(const Tune *t, uint32_t *w)
 bool valid(const Tune &t)
 {
     return (t.warps == 2 || t.warps == 4 || t.warps == 8) && (t.pool >= 1 && t.pool <= 4) && t.cta_units <= 1 &&
-           t.ring_slack <= (1u << 20);
+           t.ring_bias >= -(1 << 20) && t.ring_bias <= (1 << 20);
 }
 
 }  // namespace
@@ -197,9 +198,9 @@ extern "C" vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table
             const double rate = measure(*c, gs, t, slice_s, wide);
             if (rate > best_rate) { best_rate = rate; best = t; }
         }
-        for (uint32_t slack : {4u, 32u}) {  // then the ring threshold, with the best shape
+        for (int32_t bias : {-64, -16, 4, 32}) {  // then the ring threshold, with the best shape
             Tune t = best;
-            t.ring_slack = slack;
+            t.ring_bias = bias;
             const double rate = measure(*c, gs, t, slice_s, wide);
             if (rate > best_rate) { best_rate = rate; best = t; }
         }
@@ -225,7 +226,7 @@ extern "C" vc_status vc_set_tuning(int32_t device, const uint32_t *table, uint32
         t[i].cta_units = w[1];
         t[i].warps = w[2];
         t[i].pool = w[3];
-        t[i].ring_slack = w[4];
+        memcpy(&t[i].ring_bias, &w[4], 4);
         memcpy(&t[i].nodes_per_s, &w[5], 4);
         if (t[i].set && !valid(t[i])) return VC_ERR_INVALID;
     }

@@ -85,7 +85,8 @@ struct Params {
     uint8_t *gws;         // global workspace (CTA SUs on large graphs), else null
     unsigned long long *stats;    // per-SU counters (kStatWords each), null = off
     unsigned long long time_limit_ns;
-    uint32_t ring_slack;  // give work to the global ring only while idle CTAs exceed queued records by more than this
+    int32_t ring_bias;  // give work to the global ring while idle CTAs minus queued records exceed this (< 0: keep a surplus queued)
+    uint32_t ring_first;  // when both idle sibling warps and idle CTAs wait: 0 local pool first, 1 ring first, 2 alternate
     // server mode (persistent kernel fed by the host)
     uint32_t server;
     uint32_t subq_mask;
