@@ -150,11 +150,12 @@ vc_status vc_remove_edge_ub(const vc_csr_arena *arena, uint32_t r, int32_t devic
  * for each size class of graphs (dense n <= 64, <= 128, <= 255; wide dense
  * n <= 640; CSR n <= 1024; CSR larger) it times candidate launch shapes -- warp
  * or CTA search units, warps per CTA, CTA pool slots (the shared-memory stack
- * of donated subtrees) per warp, and the global-ring donation threshold -- on
- * seeded calibration graphs of the class for slice_s seconds each (0 = 0.3 s;
- * about 15 s in all) and installs the fastest for the device's later solves.
- * table (optional, at least 36 words) receives per class: set, cta_units,
- * warps, pool slots per warp, ring threshold, tree nodes/s (float bits).
+ * of donated subtrees) per warp, the global-ring donation threshold and the
+ * donation order -- on seeded calibration graphs of the class for slice_s
+ * seconds each (0 = 0.3 s; about 15 s in all) and installs the fastest for the
+ * device's later solves.  table (optional, at least 42 words) receives per
+ * class: set, cta_units, warps, pool slots per warp, ring threshold (int32),
+ * tree nodes/s (float bits), ring first.
  * vc_set_tuning installs such a table (e.g. saved from an earlier run); a class
  * with set = 0 uses the built-in rules. */
 vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table, uint32_t max_words);

@@ -57,6 +57,7 @@ struct Tune {
     uint32_t warps = 8;       // warps (search units) per CTA: 2, 4 or 8
     uint32_t pool = 2;        // CTA pool slots (donated subtrees) per warp: 1, 2 or 4
     int32_t ring_bias = 0;    // global-ring donations while idle CTAs minus queued records exceed this
+    uint32_t ring_first = 0;  // 1: when a sibling warp and another CTA both wait, the ring gets the subtree
     float nodes_per_s = 0;    // what the calibration measured with this choice
 };
 

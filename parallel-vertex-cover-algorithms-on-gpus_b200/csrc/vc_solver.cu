@@ -475,12 +475,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     double tl = job.time_limit_s > 0 ? job.time_limit_s : 300.0;
     P.time_limit_ns = (unsigned long long)(tl * 1e9);
     P.ring_bias = po.tune ? po.tune->ring_bias : 0;
-#ifdef VC_RING_BIAS
-    if (!po.tune) P.ring_bias = VC_RING_BIAS;
-#endif
-#ifdef VC_RING_FIRST
-    P.ring_first = VC_RING_FIRST;
-#endif
+    P.ring_first = po.tune ? po.tune->ring_first : 0u;
 
     void *args[] = {&P};
     cudaEventRecord(c.ev0, stream);

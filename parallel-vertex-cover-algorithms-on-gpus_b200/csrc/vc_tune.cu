@@ -15,6 +15,8 @@
 //   * the ring threshold: work goes to the global ring while idle CTAs minus
 //     the records already queued exceed -64, -16, 0, 4 or 32 (a negative
 //     threshold keeps a surplus of records queued for CTAs that go idle),
+//   * the donation order when an idle sibling warp and an idle CTA both wait:
+//     the CTA pool first, or the ring first,
 // on seeded calibration graphs of the class (G(n, p) of the batched family's
 // degrees, sizes spread over the class), each candidate timed for a fixed time
 // slice, and installs the winner in the device's table; later solves of that
@@ -139,32 +141,35 @@ double measure(Ctx &c, const std::vector<CalGraph> &gs, const Tune &cand, double
     return job.kernel_ms > 0 ? nodes / (job.kernel_ms * 1e-3) : -1;
 }
 
+constexpr uint32_t kTuneWords = 7;  // per class
+
 void pack(const Tune *t, uint32_t *w)
 {
     for (int i = 0; i < kTuneClasses; ++i) {
-        uint32_t *o = w + 6 * i;
+        uint32_t *o = w + kTuneWords * i;
         o[0] = t[i].set;
         o[1] = t[i].cta_units;
         o[2] = t[i].warps;
         o[3] = t[i].pool;
         memcpy(&o[4], &t[i].ring_bias, 4);
         memcpy(&o[5], &t[i].nodes_per_s, 4);
+        o[6] = t[i].ring_first;
     }
 }
 
 bool valid(const Tune &t)
 {
     return (t.warps == 2 || t.warps == 4 || t.warps == 8) && (t.pool >= 1 && t.pool <= 4) && t.cta_units <= 1 &&
-           t.ring_bias >= -(1 << 20) && t.ring_bias <= (1 << 20);
+           t.ring_bias >= -(1 << 20) && t.ring_bias <= (1 << 20) && t.ring_first <= 1;
 }
 
 }  // namespace
 
 // Measures launch shapes per size class on this device and installs the
 // fastest (see the file comment).  slice_s is the time each candidate runs
-// (0 = 0.3 s); about a dozen candidates per class.  table (optional, 36 words)
+// (0 = 0.3 s); about a dozen candidates per class.  table (optional, 42 words)
 // receives the chosen shapes: per class set, cta_units, warps, pool slots per
-// warp, ring threshold, measured tree nodes/s (float bits).
+// warp, ring threshold (int32), measured tree nodes/s (float bits), ring first.
 extern "C" vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table, uint32_t max_words)
 {
     DeviceGuard dg;
@@ -204,12 +209,18 @@ extern "C" vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table
             const double rate = measure(*c, gs, t, slice_s, wide);
             if (rate > best_rate) { best_rate = rate; best = t; }
         }
+        {  // then the donation order
+            Tune t = best;
+            t.ring_first = 1;
+            const double rate = measure(*c, gs, t, slice_s, wide);
+            if (rate > best_rate) { best_rate = rate; best = t; }
+        }
         if (best_rate <= 0) return VC_ERR_CUDA;
         best.nodes_per_s = (float)best_rate;
         best_all[k] = best;
     }
     for (int k = 0; k < kTuneClasses; ++k) c->tune[k] = best_all[k];
-    if (table && max_words >= 6 * kTuneClasses) pack(c->tune, table);
+    if (table && max_words >= kTuneWords * kTuneClasses) pack(c->tune, table);
     return VC_OK;
 }
 
@@ -218,16 +229,17 @@ extern "C" vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table
 extern "C" vc_status vc_set_tuning(int32_t device, const uint32_t *table, uint32_t words)
 {
     DeviceGuard dg;
-    if (!table || words < 6 * kTuneClasses) return VC_ERR_INVALID;
+    if (!table || words < kTuneWords * kTuneClasses) return VC_ERR_INVALID;
     Tune t[kTuneClasses];
     for (int i = 0; i < kTuneClasses; ++i) {
-        const uint32_t *w = table + 6 * i;
+        const uint32_t *w = table + kTuneWords * i;
         t[i].set = w[0] ? 1 : 0;
         t[i].cta_units = w[1];
         t[i].warps = w[2];
         t[i].pool = w[3];
         memcpy(&t[i].ring_bias, &w[4], 4);
         memcpy(&t[i].nodes_per_s, &w[5], 4);
+        t[i].ring_first = w[6];
         if (t[i].set && !valid(t[i])) return VC_ERR_INVALID;
     }
     vc_status err;

@@ -289,24 +289,28 @@ def kernel_launches() -> int:
 TUNE_CLASSES = ["dense n<=64", "dense n<=128", "dense n<=255", "wide dense n<=640", "csr n<=1024", "csr n>1024"]
 
 
+TUNE_WORDS = 7  # per class
+
+
 def _unpack_tuning(buf: np.ndarray) -> List[dict]:
     out = []
     for i, name in enumerate(TUNE_CLASSES):
-        w = buf[6 * i:6 * i + 6]
+        w = buf[TUNE_WORDS * i:TUNE_WORDS * (i + 1)]
         out.append({"class": name, "set": int(w[0]), "units": "cta" if w[1] else "warp", "warps": int(w[2]),
-                    "pool_per_warp": int(w[3]), "ring_slack": int(w[4]),
-                    "nodes_per_s": float(np.frombuffer(np.uint32(w[5]).tobytes(), dtype=np.float32)[0])})
+                    "pool_per_warp": int(w[3]), "ring_bias": int(np.uint32(w[4]).astype(np.int32)),
+                    "nodes_per_s": float(np.frombuffer(np.uint32(w[5]).tobytes(), dtype=np.float32)[0]),
+                    "ring_first": int(w[6])})
     return out
 
 
 def autotune(slice_s: float = 0.0, device: int = -1):
     """vc_autotune: measure launch shapes per size class on the device and install
     the fastest.  Returns (status, table words, readable table)."""
-    buf = np.zeros(36, dtype=np.uint32)
+    buf = np.zeros(TUNE_WORDS * len(TUNE_CLASSES), dtype=np.uint32)
     L = lib()
     L.vc_autotune.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_uint32]
     L.vc_autotune.restype = ctypes.c_int
-    st = L.vc_autotune(device, slice_s, buf.ctypes.data, 36)
+    st = L.vc_autotune(device, slice_s, buf.ctypes.data, int(buf.size))
     return st, buf, _unpack_tuning(buf)
 
 

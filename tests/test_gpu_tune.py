@@ -25,7 +25,7 @@ def test_autotune_installs_valid_shapes_and_answers_stay_exact():
         assert st == vcgpu.VC_OK
         for row in table:
             assert row["set"] == 1 and row["warps"] in (2, 4, 8) and row["pool_per_warp"] in (1, 2, 4)
-            assert row["nodes_per_s"] > 0 and row["ring_slack"] in (0, 4, 32)
+            assert row["nodes_per_s"] > 0 and row["ring_bias"] in (-64, -16, 0, 4, 32) and row["ring_first"] in (0, 1)
         recs = _golden(500_000, 120)
         graphs = [W.batch_instance(r["i"]) for r in recs]
         rng = np.random.default_rng(5)
@@ -41,4 +41,4 @@ def test_autotune_installs_valid_shapes_and_answers_stay_exact():
         bad[2] = 3  # warps must be 2, 4 or 8
         assert vcgpu.set_tuning(bad) == vcgpu.VC_ERR_INVALID
     finally:
-        assert vcgpu.set_tuning(np.zeros(36, dtype=np.uint32)) == vcgpu.VC_OK
+        assert vcgpu.set_tuning(np.zeros(vcgpu.TUNE_WORDS * len(vcgpu.TUNE_CLASSES), dtype=np.uint32)) == vcgpu.VC_OK
