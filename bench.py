@@ -77,7 +77,9 @@ def parse(argv=None):
     ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub", "profile"])
     ap.add_argument("--count", type=int, default=128)
     ap.add_argument("--reps", type=int, default=1)
-    ap.add_argument("--case", default="batch", choices=["batch", "csr-batch", "powergrid"])
+    ap.add_argument("--case", default="batch", choices=["batch", "csr-batch", "powergrid", "file"])
+    ap.add_argument("--file", default="Power-Grid.txt",
+                    help="--case file: one of the reference's graph files staged by `make -C oracle graphs`")
     ap.add_argument("--set", default="pinned", choices=["pinned", "full"])
     ap.add_argument("--time-limit", type=float, default=600.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -707,13 +709,16 @@ def ub_arm(args, world, rank):
 def profile_arm(args):
     """Small torch-free launches for ncu.  --case batch: the first --count graphs
     of the step's set in one vc_solve_batch call (the dense kernel); csr-batch:
-    the same graphs with the CSR kernel forced; powergrid: the reference's
-    Power-Grid file (n = 4942, staged by `make -C oracle graphs`), one vc_solve
-    (the CSR kernel with CTA search units).  --reps times each."""
+    the same graphs with the CSR kernel forced; file: one of the reference's
+    graph files (--file, staged by `make -C oracle graphs`; the formated_* and
+    lastfm files are 0-based), one vc_solve; powergrid: --case file on
+    Power-Grid (n = 4942, the CSR kernel with CTA search units).  --reps times
+    each."""
     import vcgpu
-    if args.case == "powergrid":
-        path = os.path.join(REPO, "oracle", "_ref", "graphs", "Power-Grid.txt.gz")
-        g = W.read_reference_file(path)
+    if args.case in ("powergrid", "file"):
+        name = "Power-Grid.txt" if args.case == "powergrid" else args.file
+        path = os.path.join(REPO, "oracle", "_ref", "graphs", name + ".gz")
+        g = W.read_reference_file(path, one_based=not (name.startswith("formated_") or name.startswith("lastfm")))
         for it in range(args.reps):
             r = vcgpu.solve(g, "mvc", time_limit=args.time_limit)
             print(f"rep {it}: status {r.status} size {r.size} tree nodes {r.tree_nodes} kernel {r.kernel_ms:.1f} ms "

@@ -142,6 +142,7 @@ struct PlanOpts {
     bool wide = false;         // graphs of 256..640 vertices may take the wide dense kernel
     bool warp_gws = false;     // warp units with global-memory workspaces
     bool lanes = false;        // graphs <= 255 vertices take the lane kernel
+    bool team = false;         // CSR kernels walk rows with teams of lanes (average degree >= 4)
     const Tune *tune = nullptr; // the size class's tuned shape, if any
 };
 

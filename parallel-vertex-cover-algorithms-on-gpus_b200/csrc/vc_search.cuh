@@ -147,6 +147,7 @@ struct WarpG {
     __device__ __forceinline__ static unsigned su_global() { return blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); }
     __device__ __forceinline__ static unsigned warp() { return 0; }
     static constexpr unsigned kWarps = 1;
+    static constexpr bool kTeam = false;  // CSR rows walked one lane per row
 };
 
 template <unsigned NT>
@@ -200,6 +201,14 @@ struct BlockG {
     __device__ __forceinline__ static unsigned su_local() { return 0; }
     __device__ __forceinline__ static unsigned su_global() { return blockIdx.x; }
     __device__ __forceinline__ static unsigned warp() { return threadIdx.x >> 5; }
+    static constexpr bool kTeam = false;
+};
+
+// The same group with CSR rows walked by teams of lanes (see Team): the choice
+// for graphs whose average degree is 4 or more.
+template <class Base>
+struct TeamG : Base {
+    static constexpr bool kTeam = true;
 };
 
 // ---------------------------------------------------------------- SU state
@@ -223,9 +232,42 @@ struct SU {
     bool cg;          // graph reads around L1 (server launches)
     uint32_t c_best;  // cached incumbent (refreshed every few nodes; stale values only weaken pruning)
     uint32_t fr_bot, fr_top;
+    uint32_t tlg;   // log2 of the lanes that walk one CSR row together (see Team)
     unsigned long long local_nodes;
     unsigned long long deadline;
 };
+
+// A team: 2^lg consecutive lanes of one warp that walk one CSR row together
+// (coalesced loads, lane j reads entries j, j + w, ...), while the group's other
+// teams work on other vertices.  The width follows the graph's average degree:
+// one lane per row where rows are a few entries long, the whole warp where they
+// are hundreds long.  Teams never straddle a warp, so their ballots, shuffles
+// and reductions use the team's own lane mask.
+// The members are recomputed from lg where used (a few integer operations) so
+// that they hold no registers across the walks.
+template <class G>
+struct Team {
+    uint32_t lg;
+    __device__ __forceinline__ uint32_t w() const { return 1u << lg; }
+    __device__ __forceinline__ uint32_t lane() const { return G::rank() & (w() - 1u); }
+    __device__ __forceinline__ uint32_t id() const { return G::rank() >> lg; }
+    __device__ __forceinline__ uint32_t T() const { return G::kSize >> lg; }
+    __device__ __forceinline__ uint32_t src() const { return threadIdx.x & 31u & ~(w() - 1u); }
+    __device__ __forceinline__ uint32_t mask() const
+    {
+        return lg == 5u ? 0xffffffffu : ((1u << w()) - 1u) << src();
+    }
+};
+
+// Team width for a graph of n vertices and m2 = 2m CSR entries: one lane below
+// an average degree of 4 (rows of two or three entries keep 32 vertices in
+// flight per warp), else the largest power of two not above the average
+// degree, up to the whole warp.
+__device__ __forceinline__ uint32_t team_lg(uint32_t n, uint32_t m2)
+{
+    const uint32_t avg = n ? m2 / n : 0u;
+    return avg < 4u ? 0u : min(5u, 31u - (uint32_t)__clz(avg));
+}
 
 // The record bitmap a search unit fills for donation (see donation_bits).
 __device__ __forceinline__ uint32_t *rec_bits(SU &s) { return s.bits; }
@@ -260,16 +302,37 @@ __device__ __forceinline__ bool row_contains(bool cg, const uint32_t *rp, const 
 }
 
 // One thread takes v: claim it, log it on the trail, decrement live neighbours.
-__device__ __forceinline__ void take_one(SU &s, uint32_t v)
+__device__ __forceinline__ void take_one_lane(SU &s, uint32_t v)
 {
-    int32_t old = atomicExch(&s.deg[v], kDead);
+    const int32_t old = atomicExch(&s.deg[v], kDead);
     if (old < 0) return;
-    uint32_t idx = atomicAdd(&s.ctr[0], 1u);
-    s.trail[idx] = v;
+    s.trail[atomicAdd(&s.ctr[0], 1u)] = v;
     volatile int32_t *dv = s.deg;
-    uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+    const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
     for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
-        uint32_t u = gld(s.cg, &s.cl[e]);
+        const uint32_t u = gld(s.cg, &s.cl[e]);
+        if (dv[u] >= 0) atomicSub(&s.deg[u], 1);
+    }
+}
+
+// One team takes v: its first lane claims v and logs it on the trail, then the
+// team decrements v's live neighbours.
+template <class G>
+__device__ __forceinline__ void take_one(SU &s, uint32_t v, const Team<G> &t)
+{
+    uint32_t ok = 0;
+    if (t.lane() == 0) {
+        const int32_t old = atomicExch(&s.deg[v], kDead);
+        if (old >= 0) {
+            s.trail[atomicAdd(&s.ctr[0], 1u)] = v;
+            ok = 1;
+        }
+    }
+    if (!__shfl_sync(t.mask(), ok, t.src())) return;
+    volatile int32_t *dv = s.deg;
+    const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+    for (uint32_t e = gld(s.cg, &s.rp[v]) + t.lane(); e < e1; e += t.w()) {
+        const uint32_t u = gld(s.cg, &s.cl[e]);
         if (dv[u] >= 0) atomicSub(&s.deg[u], 1);
     }
 }
@@ -307,31 +370,73 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
     const uint32_t nc = s.ctr[1];
     G::sync();
     if (G::rank() == 0) s.ctr[1] = 0;
-    for (uint32_t i = G::rank(); i < nc; i += G::kSize) {
+    const Team<G> t{s.tlg};
+    if constexpr (!G::kTeam) {  // rows of a few entries: a lane per candidate
+        for (uint32_t i = G::rank(); i < nc; i += G::kSize) {
+            const uint32_t v = s.cand[i];
+            if (deg[v] == 1) {        // degree-one rule (helperFunctions.cuh:252-265)
+                const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+                for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+                    const uint32_t u = gld(s.cg, &s.cl[e]);
+                    const int32_t du = deg[u];
+                    if (du > 0) {
+                        if (du > 1 || u < v) { mark(s.marks, u); marked = true; }
+                        break;
+                    }
+                }
+            } else {                  // degree-two triangle rule (helperFunctions.cuh:384-417)
+                uint32_t n1 = kNone, n2 = kNone;
+                bool keep = false;
+                const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+                for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+                    const uint32_t u = gld(s.cg, &s.cl[e]);
+                    const int32_t du = deg[u];
+                    if (du > 0) {
+                        if (du == 1 || (du == 2 && u < v)) { keep = true; break; }
+                        if (n1 == kNone) n1 = u; else { n2 = u; break; }
+                    }
+                }
+                if (!keep && n2 != kNone && row_contains(s.cg, s.rp, s.cl, n2, n1)) {
+                    mark(s.marks, n1);
+                    mark(s.marks, n2);
+                    marked = true;
+                }
+            }
+        }
+    }
+    // Otherwise a team per candidate finds its live neighbours in row order
+    // (degrees do not change during this loop, so a degree-d vertex has exactly
+    // d of them); the same rules on them.
+    for (uint32_t i = G::kTeam ? t.id() : nc; i < nc; i += t.T()) {
         const uint32_t v = s.cand[i];
-        if (deg[v] == 1) {        // degree-one rule (helperFunctions.cuh:252-265)
-            uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
-            for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
-                uint32_t u = gld(s.cg, &s.cl[e]);
-                int32_t du = deg[u];
-                if (du > 0) {
-                    if (du > 1 || u < v) { mark(s.marks, u); marked = true; }
-                    break;
-                }
+        const uint32_t dv0 = (uint32_t)deg[v];  // 1 or 2
+        uint32_t got = 0, n1 = kNone, n2 = kNone;
+        int32_t d1 = 0, d2 = 0;
+        const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+        for (uint32_t eb = gld(s.cg, &s.rp[v]); eb < e1 && got < dv0; eb += t.w()) {
+            const uint32_t e = eb + t.lane();
+            uint32_t u = kNone;
+            int32_t du = 0;
+            if (e < e1) {
+                u = gld(s.cg, &s.cl[e]);
+                du = deg[u];
             }
-        } else {                  // degree-two triangle rule (helperFunctions.cuh:384-417)
-            uint32_t n1 = kNone, n2 = kNone;
-            bool keep = false;
-            uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
-            for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
-                uint32_t u = gld(s.cg, &s.cl[e]);
-                int32_t du = deg[u];
-                if (du > 0) {
-                    if (du == 1 || (du == 2 && u < v)) { keep = true; break; }
-                    if (n1 == kNone) n1 = u; else { n2 = u; break; }
-                }
+            uint32_t live = __ballot_sync(t.mask(), du > 0) >> t.src();
+            while (live && got < dv0) {
+                const uint32_t b = __ffs(live) - 1;
+                live &= live - 1;
+                const uint32_t uu = __shfl_sync(t.mask(), u, t.src() + b);
+                const int32_t dd = __shfl_sync(t.mask(), du, t.src() + b);
+                if (got == 0) { n1 = uu; d1 = dd; } else { n2 = uu; d2 = dd; }
+                ++got;
             }
-            if (!keep && n2 != kNone && row_contains(s.cg, s.rp, s.cl, n2, n1)) {
+        }
+        if (t.lane() != 0 || n1 == kNone) continue;
+        if (dv0 == 1) {           // degree-one rule (helperFunctions.cuh:252-265)
+            if (d1 > 1 || n1 < v) { mark(s.marks, n1); marked = true; }
+        } else if (n2 != kNone) { // degree-two triangle rule (helperFunctions.cuh:384-417)
+            const bool keep = d1 == 1 || (d1 == 2 && n1 < v) || d2 == 1 || (d2 == 2 && n2 < v);
+            if (!keep && row_contains(s.cg, s.rp, s.cl, n2, n1)) {
                 mark(s.marks, n1);
                 mark(s.marks, n2);
                 marked = true;
@@ -341,17 +446,35 @@ __device__ __forceinline__ bool reduce_pass(SU &s, uint32_t del, uint32_t bound,
     s.stat.passes += 1;
     if (G::any(marked)) {
         G::sync();  // the vote is not a memory barrier: make every lane's marks visible
-        for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) {
-            uint32_t m = s.marks[w];
-            if (!m) continue;
-            s.marks[w] = 0;
-            while (m) {
-                uint32_t b = __ffs(m) - 1;
-                m &= m - 1;
-                take_one(s, w * 32 + b);
+        if constexpr (!G::kTeam) {  // a lane per marks word takes its vertices
+            for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) {
+                uint32_t m = s.marks[w];
+                if (!m) continue;
+                s.marks[w] = 0;
+                while (m) {
+                    const uint32_t b = __ffs(m) - 1;
+                    m &= m - 1;
+                    take_one_lane(s, w * 32 + b);
+                }
             }
+            G::sync();
+        } else {  // list the marked vertices (the candidate list is spent), then a team takes each
+            for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) {
+                uint32_t m = s.marks[w];
+                if (!m) continue;
+                s.marks[w] = 0;
+                uint32_t at = atomicAdd(&s.ctr[3], (uint32_t)__popc(m));
+                while (m) {
+                    s.cand[at++] = w * 32 + __ffs(m) - 1;
+                    m &= m - 1;
+                }
+            }
+            G::sync();
+            const uint32_t nm = s.ctr[3];
+            for (uint32_t i = t.id(); i < nm; i += t.T()) take_one(s, s.cand[i], t);
+            G::sync();
+            if (G::rank() == 0) s.ctr[3] = 0;  // every thread read it before the barrier; the next use is a pass later
         }
-        G::sync();
         return true;
     }
     o.sum = G::sum(sum);
@@ -389,8 +512,13 @@ __device__ __forceinline__ void take_vertex(SU &s, uint32_t v)
 template <class G>
 __device__ __forceinline__ void take_neighbours(SU &s, uint32_t v)
 {
-    uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
-    for (uint32_t e = gld(s.cg, &s.rp[v]) + G::rank(); e < e1; e += G::kSize) take_one(s, gld(s.cg, &s.cl[e]));
+    const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+    if constexpr (G::kTeam) {
+        const Team<G> t{s.tlg};
+        for (uint32_t e = gld(s.cg, &s.rp[v]) + t.id(); e < e1; e += t.T()) take_one(s, gld(s.cg, &s.cl[e]), t);
+    } else {
+        for (uint32_t e = gld(s.cg, &s.rp[v]) + G::rank(); e < e1; e += G::kSize) take_one_lane(s, gld(s.cg, &s.cl[e]));
+    }
     G::sync();
 }
 
@@ -404,17 +532,36 @@ __device__ __forceinline__ void restore_to(SU &s, uint32_t pos)
     for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) s.deg[s.trail[i]] = kRestoring;
     G::sync();
     volatile int32_t *dv = s.deg;
-    for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {
-        uint32_t v = s.trail[i];
-        uint32_t c = 0;
-        uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
-        for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
-            uint32_t u = gld(s.cg, &s.cl[e]);
-            int32_t d = dv[u];
-            if (d == kRestoring) ++c;
-            else if (d >= 0) { atomicAdd(&s.deg[u], 1); ++c; }
+    if constexpr (G::kTeam) {
+        const Team<G> t{s.tlg};
+        for (uint32_t i = pos + t.id(); i < top; i += t.T()) {  // a team per trail vertex
+            const uint32_t v = s.trail[i];
+            uint32_t c = 0;
+            const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+            for (uint32_t e = gld(s.cg, &s.rp[v]) + t.lane(); e < e1; e += t.w()) {
+                const uint32_t u = gld(s.cg, &s.cl[e]);
+                const int32_t d = dv[u];
+                if (d == kRestoring) ++c;
+                else if (d >= 0) { atomicAdd(&s.deg[u], 1); ++c; }
+            }
+            c = __reduce_add_sync(t.mask(), c);  // every lane of the team has read trail[i]
+            if (t.lane() == 0) {
+                if (s.aux) s.aux[i] = c; else s.trail[i] = v | (c << 16);
+            }
         }
-        if (s.aux) s.aux[i] = c; else s.trail[i] = v | (c << 16);
+    } else {
+        for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {  // a lane per trail vertex
+            const uint32_t v = s.trail[i];
+            uint32_t c = 0;
+            const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+            for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
+                const uint32_t u = gld(s.cg, &s.cl[e]);
+                const int32_t d = dv[u];
+                if (d == kRestoring) ++c;
+                else if (d >= 0) { atomicAdd(&s.deg[u], 1); ++c; }
+            }
+            if (s.aux) s.aux[i] = c; else s.trail[i] = v | (c << 16);
+        }
     }
     G::sync();
     for (uint32_t i = pos + G::rank(); i < top; i += G::kSize) {
@@ -446,22 +593,24 @@ template <class G>
 __device__ __forceinline__ void rebuild(SU &s)
 {
     uint32_t pad_end = s.nw * 32;
-    for (uint32_t v = G::rank(); v < pad_end; v += G::kSize) {
-        if (v >= s.n) { s.deg[v] = 0; continue; }
-        if ((s.bits[v >> 5] >> (v & 31u)) & 1u) { s.deg[v] = kDead; continue; }
+    const Team<G> t{G::kTeam ? s.tlg : 0u};  // a team (or a lane) per vertex
+    for (uint32_t v = t.id(); v < pad_end; v += t.T()) {
+        if (v >= s.n) { if (t.lane() == 0) s.deg[v] = 0; continue; }
+        if ((s.bits[v >> 5] >> (v & 31u)) & 1u) { if (t.lane() == 0) s.deg[v] = kDead; continue; }
         uint32_t c = 0;
-        uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
-        for (uint32_t e = gld(s.cg, &s.rp[v]); e < e1; ++e) {
-            uint32_t u = gld(s.cg, &s.cl[e]);
+        const uint32_t e1 = gld(s.cg, &s.rp[v + 1]);
+        for (uint32_t e = gld(s.cg, &s.rp[v]) + t.lane(); e < e1; e += t.w()) {
+            const uint32_t u = gld(s.cg, &s.cl[e]);
             c += ((s.bits[u >> 5] >> (u & 31u)) & 1u) ^ 1u;
         }
-        s.deg[v] = (int32_t)c;
+        if constexpr (G::kTeam) c = __reduce_add_sync(t.mask(), c);
+        if (t.lane() == 0) s.deg[v] = (int32_t)c;
     }
     uint32_t pc = 0;
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) pc += __popc(s.bits[w]);
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
     s.base_del = G::sum(pc);
-    if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; }
+    if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; s.ctr[3] = 0; }
     G::sync();
 }
 
@@ -478,6 +627,7 @@ __device__ __forceinline__ void bind_graph(SU &s, const Params &P, uint32_t inst
     s.node_limit = d.node_limit;
     s.rp = P.row_ptr + d.row_off;
     s.cl = P.col + d.col_off;
+    s.tlg = team_lg(d.n, gld(s.cg, &s.rp[d.n]));
     s.fr_bot = s.fr_top = 0;
     s.local_nodes = 0;
 }
@@ -491,7 +641,7 @@ __device__ __forceinline__ void load_root(SU &s)
         s.deg[v] = v < s.n ? (int32_t)(gld(s.cg, &s.rp[v + 1]) - gld(s.cg, &s.rp[v])) : 0;
     for (uint32_t w = G::rank(); w < s.nw; w += G::kSize) s.marks[w] = 0;
     s.base_del = 0;
-    if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; }
+    if (G::rank() == 0) { s.ctr[0] = 0; s.ctr[1] = 0; s.ctr[3] = 0; }
     G::sync();
 }
 

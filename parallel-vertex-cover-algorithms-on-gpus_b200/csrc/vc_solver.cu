@@ -30,13 +30,16 @@ std::atomic<uint64_t> g_launches{0};
 
 // Resident threads per SM the search kernels are register-limited for
 // (1024 -> at most 64 registers per thread, 32 warps per SM).
+// Team-walk kernels also come with 768 (80 registers), taken where the extra
+// registers cost no resident CTAs (see plan_variant).
 #ifndef VC_MIN_THREADS_PER_SM
 #define VC_MIN_THREADS_PER_SM 1024
 #endif
+constexpr unsigned kRoomyThreadsPerSM = 768;
 
 // ---------------------------------------------------------------- kernels
-template <class G, unsigned NT>
-__global__ void __launch_bounds__(NT, VC_MIN_THREADS_PER_SM / NT) k_search(Params P)
+template <class G, unsigned NT, unsigned MinThreads = VC_MIN_THREADS_PER_SM>
+__global__ void __launch_bounds__(NT, MinThreads / NT) k_search(Params P)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint32_t cp_hdr[kCpHdrWords];
@@ -214,42 +217,47 @@ Ctx *get_ctx(int dev, vc_status *err)
 }
 
 // ---------------------------------------------------------------- sizing
-template <class G, unsigned NT>
-static cudaError_t plan_variant(Ctx &c, Plan &pl, uint32_t smem_per_block)
+// Resident CTAs per SM of `fn` with `smem` bytes of dynamic shared memory (0 on error).
+template <unsigned NT, class F>
+static int ctas_per_sm(F fn, uint32_t smem)
 {
-    auto fn = k_search<G, NT>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_per_block);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)NT, smem_per_block);
-    if (e != cudaSuccess) return e;
-    if (per_sm <= 0) return cudaErrorInvalidConfiguration;
-    pl.fn = (const void *)fn;
-    pl.block = NT;
-    pl.grid = (uint32_t)per_sm * (uint32_t)c.sms;
-    pl.smem = smem_per_block;
-    return cudaSuccess;
-}
-
-static uint32_t cta_pool_bytes(uint32_t slots, uint32_t stride)
-{
-    return slots ? 4u * ((slots + 3) / 4 * 4) + 4u * slots * stride : 0u;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)NT, smem) != cudaSuccess)
+        return 0;
+    return per_sm;
 }
 
 template <unsigned NT, class F>
 static cudaError_t plan_variant_fn(Ctx &c, Plan &pl, uint32_t smem_per_block, F fn)
 {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_per_block);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)NT, smem_per_block);
-    if (e != cudaSuccess) return e;
+    const int per_sm = ctas_per_sm<NT>(fn, smem_per_block);
     if (per_sm <= 0) return cudaErrorInvalidConfiguration;
     pl.fn = (const void *)fn;
     pl.block = NT;
     pl.grid = (uint32_t)per_sm * (uint32_t)c.sms;
     pl.smem = smem_per_block;
     return cudaSuccess;
+}
+
+// The CSR kernel for group G: team-walk kernels take the 80-register build
+// when shared memory already holds the SM to as few CTAs (their row walks
+// keep more values live than the lane walks).
+template <class G, unsigned NT>
+static cudaError_t plan_variant(Ctx &c, Plan &pl, uint32_t smem_per_block)
+{
+    if constexpr (G::kTeam) {
+        auto roomy = k_search<G, NT, kRoomyThreadsPerSM>;
+        const int r = ctas_per_sm<NT>(roomy, smem_per_block);
+        if (r > 0 && r >= ctas_per_sm<NT>(k_search<G, NT>, smem_per_block))
+            return plan_variant_fn<NT>(c, pl, smem_per_block, roomy);
+    }
+    return plan_variant_fn<NT>(c, pl, smem_per_block, k_search<G, NT>);
+}
+
+static uint32_t cta_pool_bytes(uint32_t slots, uint32_t stride)
+{
+    return slots ? 4u * ((slots + 3) / 4 * 4) + 4u * slots * stride : 0u;
 }
 
 // Chooses the search-unit shape for a vertex capacity np: one warp per SU with
@@ -303,6 +311,18 @@ static cudaError_t plan_lanes(Ctx &c, Plan &pl, uint32_t nmax)
     return cudaSuccess;
 }
 
+// Warp units, `warps` to a CTA.
+template <class G>
+static cudaError_t plan_warps(Ctx &c, Plan &pl, uint32_t warps, uint32_t smem)
+{
+    switch (warps) {
+    case 8: return plan_variant<G, 256>(c, pl, smem);
+    case 4: return plan_variant<G, 128>(c, pl, smem);
+    case 2: return plan_variant<G, 64>(c, pl, smem);
+    default: return plan_variant<G, 32>(c, pl, smem);
+    }
+}
+
 cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOpts &o)
 {
     pl.dense = false;
@@ -338,13 +358,7 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
         uint32_t warps = t ? t->warps : (o.warps ? o.warps : 8);
         pl.cta_slots = warps > 1 ? per_warp * warps : 0;
         const uint32_t smem = cta_pool_bytes(pl.cta_slots, pl.stride);
-        cudaError_t e;
-        switch (warps) {
-        case 8: e = plan_variant<WarpG, 256>(c, pl, smem); break;
-        case 4: e = plan_variant<WarpG, 128>(c, pl, smem); break;
-        case 2: e = plan_variant<WarpG, 64>(c, pl, smem); break;
-        default: e = plan_variant<WarpG, 32>(c, pl, smem); break;
-        }
+        cudaError_t e = o.team ? plan_warps<TeamG<WarpG>>(c, pl, warps, smem) : plan_warps<WarpG>(c, pl, warps, smem);
         if (e != cudaSuccess) return e;
         pl.num_su = pl.grid * (pl.block / 32);
         pl.global_ws = true;
@@ -356,13 +370,7 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
         if (warps * pl.su_bytes + cta_pool_bytes(warps > 1 ? per_warp * warps : 0, pl.stride) <= budget) {
             pl.cta_slots = warps > 1 ? per_warp * warps : 0;
             uint32_t smem = warps * pl.su_bytes + cta_pool_bytes(pl.cta_slots, pl.stride);
-            cudaError_t e;
-            switch (warps) {
-            case 8: e = plan_variant<WarpG, 256>(c, pl, smem); break;
-            case 4: e = plan_variant<WarpG, 128>(c, pl, smem); break;
-            case 2: e = plan_variant<WarpG, 64>(c, pl, smem); break;
-            default: e = plan_variant<WarpG, 32>(c, pl, smem); break;
-            }
+            cudaError_t e = o.team ? plan_warps<TeamG<WarpG>>(c, pl, warps, smem) : plan_warps<WarpG>(c, pl, warps, smem);
             if (e != cudaSuccess) return e;
             pl.num_su = pl.grid * (pl.block / 32);
             pl.global_ws = false;
@@ -370,14 +378,12 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
         }
     }
     pl.cta_slots = 0;
-    if (pl.su_bytes <= budget) {
-        cudaError_t e = plan_variant<BlockG<512>, 512>(c, pl, pl.su_bytes);
+    {
+        const uint32_t smem = pl.su_bytes <= budget ? pl.su_bytes : 0u;
+        cudaError_t e = o.team ? plan_variant<TeamG<BlockG<512>>, 512>(c, pl, smem)
+                               : plan_variant<BlockG<512>, 512>(c, pl, smem);
         if (e != cudaSuccess) return e;
-        pl.global_ws = false;
-    } else {
-        cudaError_t e = plan_variant<BlockG<512>, 512>(c, pl, 0);
-        if (e != cudaSuccess) return e;
-        pl.global_ws = true;
+        pl.global_ws = smem == 0;
     }
     pl.num_su = pl.grid;
     return cudaSuccess;
@@ -400,15 +406,18 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     const uint32_t count = (uint32_t)job.desc.size();
     if (count == 0) return VC_OK;
     uint32_t nmax = 0, cover_words = 0;
+    uint64_t sum_n = 0, sum_m2 = 0;
     for (auto &d : job.desc) {
         nmax = std::max(nmax, d.n);
         d.cover_off = cover_words;
         cover_words += d.nw;
+        if (d.m2 != kNone) { sum_n += d.n; sum_m2 += d.m2; }
     }
     uint32_t np = std::max<uint32_t>(32, (nmax + 31) / 32 * 32);
     Plan pl;
     PlanOpts po;
     po.wide = job.wide;
+    po.team = sum_m2 >= 4 * sum_n && sum_n > 0;  // average degree 4 or more: rows walked by teams
     // Lane units (one thread per search unit, vc_lanes.cuh) are opt-in: they
     // execute half the instructions per tree node of warp units but, at 12
     // resident warps per SM, issue on a fifth of the cycles (ncu, batched
