@@ -1,7 +1,9 @@
 // vc_dense.cuh -- the search for graphs of at most 255 vertices (the batched
 // workload's G(n, p) instances, n in [30, 200], and the 60-vertex case), and,
 // with 20-word rows, for graphs of up to 640 vertices whose degrees all fit a
-// byte (at most 254).
+// byte (at most 254); with 16- and 32-word rows and 16-bit degrees (two to a
+// word, see "Half" below), for graphs of up to 512 and 1024 vertices of any
+// degree -- the dense DIMACS-style graphs the CSR walks handle worst.
 //
 // Same search as vc_search.cuh (the reference's degree-one, triangle and
 // high-degree rules, the E > b^2 prune and max-degree branching), with dense
@@ -35,9 +37,12 @@ namespace vcg {
 
 template <int NW>
 struct Rows {
-    static constexpr int kStride = NW == 8 ? 12 : NW;  // dense_row_words
-    static constexpr int kJ = NW >= 8 ? NW / 4 : 1;     // degree words per lane
-    static constexpr int kCandBits = 4 * kJ >= 16 ? 5 : (4 * kJ >= 8 ? 4 : 3);  // bits of a lane's candidate count
+    static constexpr bool kHalf = NW == 16 || NW == 32;  // 16-bit degrees (dense_half)
+    static constexpr int kStride = NW == 8 ? 12 : (kHalf ? NW + 4 : NW);  // dense_row_words
+    static constexpr int kPer = kHalf ? 2 : 4;                             // degrees per word
+    static constexpr int kJ = kHalf ? NW / 2 : (NW >= 8 ? NW / 4 : 1);     // degree words per lane
+    // bits of a lane's candidate count (at most kPer * kJ)
+    static constexpr int kCandBits = kPer * kJ >= 32 ? 6 : (kPer * kJ >= 16 ? 5 : (kPer * kJ >= 8 ? 4 : 3));
     static constexpr int kTri = 32 * NW * kStride;          // offset of the triangle bitmap
 };
 
@@ -52,6 +57,19 @@ __device__ __forceinline__ uint32_t spread4(uint32_t nib) { return (nib * 0x0020
 
 // The top bits of 4 bytes (bit 8b+7) -> 4 bits (bit b).
 __device__ __forceinline__ uint32_t gather4(uint32_t hb) { return ((hb >> 7) * 0x01020408u) >> 24; }
+
+// Half: the same tests on two 16-bit degrees per word (values below 2^15).
+// 0x8000 in every halfword of x that is zero, 0 elsewhere.
+__device__ __forceinline__ uint32_t halves_zero(uint32_t x)
+{
+    return ~(((x & 0x7FFF7FFFu) + 0x7FFF7FFFu) | x | 0x7FFF7FFFu);
+}
+
+// 2 bits -> the low bit of each halfword.
+__device__ __forceinline__ uint32_t spread2(uint32_t b) { return (b & 1u) | ((b & 2u) << 15); }
+
+// The top bits of 2 halfwords (bits 15, 31) -> 2 bits.
+__device__ __forceinline__ uint32_t gather2(uint32_t hb) { return ((hb >> 15) & 1u) | ((hb >> 30) & 2u); }
 
 // extra CTA header words used by the dense kernel
 enum : uint32_t { kCpStaged = 5, kCpCursorClosed = 6 };
@@ -82,8 +100,9 @@ struct DSU {
     __device__ __forceinline__ uint16_t *trail() const { return reinterpret_cast<uint16_t *>(lsm() + NW); }  // [32*NW]
     __device__ __forceinline__ uint16_t *cand() const { return trail() + 32 * NW; }   // [32*NW] pass candidates
     __device__ __forceinline__ uint8_t *degs() const { return reinterpret_cast<uint8_t *>(cand() + 32 * NW); }  // [32*NW] staging copy of D
-    uint32_t D[Rows<NW>::kJ];   // degree bytes of vertices 4q..4q+3, q = 32j + lane
-    uint32_t Ln[Rows<NW>::kJ];  // their live bits (4 per word)
+    __device__ __forceinline__ uint16_t *degs16() const { return reinterpret_cast<uint16_t *>(cand() + 32 * NW); }  // the same, Half
+    uint32_t D[Rows<NW>::kJ];   // degree bytes of vertices 4q..4q+3, q = 32j + lane (Half: 16-bit degrees of 2q, 2q+1)
+    uint32_t Ln[Rows<NW>::kJ];  // their live bits (4 per word; Half: 2)
     const uint32_t *rp, *cl;
     uint32_t inst, n, nw, mode, k, cover_off;
     unsigned long long node_limit;
@@ -147,7 +166,10 @@ __device__ __forceinline__ void live_nibbles(DSU<NW> &s)
 #pragma unroll
     for (int j = 0; j < Rows<NW>::kJ; ++j) {
         const uint32_t q = 32u * j + lane;
-        s.Ln[j] = q < 8u * s.nw ? (s.lsm()[q >> 3] >> (4u * (lane & 7u))) & 0xFu : 0u;
+        if constexpr (Rows<NW>::kHalf)
+            s.Ln[j] = q < 16u * s.nw ? (s.lsm()[q >> 4] >> (2u * (lane & 15u))) & 0x3u : 0u;
+        else
+            s.Ln[j] = q < 8u * s.nw ? (s.lsm()[q >> 3] >> (4u * (lane & 7u))) & 0xFu : 0u;
     }
 }
 
@@ -170,14 +192,16 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
 #pragma unroll
             for (int w = 0; w < NW; ++w) c += __popc(r[w] & L[w]);
         }
-        s.degs()[v] = (uint8_t)c;
+        if constexpr (Rows<NW>::kHalf) s.degs16()[v] = (uint16_t)c;
+        else s.degs()[v] = (uint8_t)c;
     }
     __syncwarp();
     const uint32_t *d32 = reinterpret_cast<const uint32_t *>(s.degs());
+    constexpr uint32_t kWordsPerLsm = 32u / Rows<NW>::kPer;  // degree words per word of L
 #pragma unroll
     for (int j = 0; j < Rows<NW>::kJ; ++j) {
         const uint32_t q = 32u * j + lane;
-        s.D[j] = q < 8u * s.nw ? d32[q] : 0u;
+        s.D[j] = q < kWordsPerLsm * s.nw ? d32[q] : 0u;
     }
     live_nibbles(s);
 }
@@ -229,8 +253,44 @@ __device__ __forceinline__ void dense_restore(DSU<NW> &s, uint32_t pos)
 // updated): subtract its edges from the degrees of the live vertices and zero
 // the bytes of the removed ones.
 template <int NW>
+__device__ __forceinline__ void dense_apply_half(DSU<NW> &s)
+{
+    constexpr int J = Rows<NW>::kJ;
+    const unsigned lane = lane_id();
+    live_nibbles(s);
+    {
+        // word 2j + lane/16 of a row holds the bits of this lane's vertices 2q, 2q+1
+        const uint32_t sh = 2u * (lane & 15u);
+        const uint32_t *rows = s.adj + (lane >> 4);
+        const uint32_t mw = lane < s.nw ? s.marks()[lane] : 0u;
+        uint32_t wm = __ballot_sync(0xffffffffu, mw != 0u);
+        uint32_t acc[J];
+#pragma unroll
+        for (int j = 0; j < J; ++j) acc[j] = 0u;
+        while (wm) {
+            const uint32_t w = __ffs(wm) - 1;
+            wm &= wm - 1;
+            uint32_t m = __shfl_sync(0xffffffffu, mw, w);
+            while (m) {
+                const uint32_t u = 32u * w + (__ffs(m) - 1);
+                m &= m - 1;
+                const uint32_t *r = rows + u * Rows<NW>::kStride;
+#pragma unroll
+                for (int j = 0; j < J; ++j) acc[j] += spread2((r[2 * j] >> sh) & s.Ln[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < J; ++j) s.D[j] = (s.D[j] - acc[j]) & (spread2(s.Ln[j]) * 0xFFFFu);
+    }
+}
+
+template <int NW>
 __device__ __forceinline__ void dense_apply(DSU<NW> &s)
 {
+    if constexpr (Rows<NW>::kHalf) {
+        dense_apply_half(s);
+        return;
+    } else {
     constexpr int J = Rows<NW>::kJ;
     const unsigned lane = lane_id();
     live_nibbles(s);
@@ -264,6 +324,7 @@ __device__ __forceinline__ void dense_apply(DSU<NW> &s)
     }
 #pragma unroll
     for (int j = 0; j < J; ++j) s.D[j] = (s.D[j] - acc[j]) & (spread4(s.Ln[j]) * 0xFFu);
+    }
 }
 
 // One reduction pass (same rules and semantics as reduce_pass in vc_search.cuh)
@@ -274,7 +335,7 @@ __device__ __forceinline__ void dense_apply(DSU<NW> &s)
 // were made (left in s.marks()); otherwise fills o with the degree sum, the
 // maximum degree and its lowest vertex.
 template <int NW>
-__device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
+__device__ __forceinline__ bool dense_pass_byte(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
 {
     constexpr int J = Rows<NW>::kJ;
     const unsigned lane = lane_id();
@@ -387,6 +448,126 @@ __device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bo
     }
     o.amax = __reduce_min_sync(0xffffffffu, first);
     return false;
+}
+
+// dense_pass on 16-bit degrees (Half): the same rules and results.
+template <int NW>
+__device__ __forceinline__ bool dense_pass_half(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
+{
+    constexpr int J = Rows<NW>::kJ;
+    const unsigned lane = lane_id();
+    const uint32_t sh = 2u * (lane & 15u);  // this lane's 2 bits in words of L, marks and tri
+    const int tt = (int)bound - (int)del;  // the high-degree rule takes deg >= tt
+    const uint32_t tl = (uint32_t)(tt > 0 ? min(tt, 0x7FFF) : 0) * 0x00010001u;
+    const uint32_t *tri = s.adj + Rows<NW>::kTri;
+    bool marked = false;
+    uint32_t cn[J], ctot = 0;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const uint32_t d = s.D[j];
+        const uint32_t q = 32u * j + lane;  // vertices 2q, 2q + 1
+        const uint32_t nz = ~halves_zero(d) & 0x80008000u;
+        // degrees are below 2^15, so 0x8000 + d - tt keeps its top bit iff d >= tt
+        const uint32_t ge = tt <= 1 ? nz : (tt >= 0x7FFF ? 0u : ((d | 0x80008000u) - tl) & 0x80008000u);
+        const uint32_t tn = (tri[q >> 4] >> sh) & 0x3u;
+        const uint32_t d12 = halves_zero(d ^ 0x00010001u) | (halves_zero(d ^ 0x00020002u) & (spread2(tn) << 15));
+        const uint32_t hn = gather2(ge);
+        if (hn) {
+            atomicOr(&s.marks()[q >> 4], hn << sh);
+            marked = true;
+        }
+        cn[j] = gather2(d12 & ~ge);
+        ctot += __popc(cn[j]);
+    }
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t pre = 0, total = 0;
+#pragma unroll
+    for (int b = 0; b < Rows<NW>::kCandBits; ++b) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
+        pre += __popc(bal & lt) << b;
+        total += __popc(bal) << b;
+    }
+    if (total) {
+        uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs16());
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const uint32_t q = 32u * j + lane;
+            if (q < 16u * s.nw) d32[q] = s.D[j];
+            uint32_t m = cn[j];
+            while (m) {
+                const uint32_t b = __ffs(m) - 1;
+                m &= m - 1;
+                s.cand()[pre++] = (uint16_t)(2u * q + b);
+            }
+        }
+        uint32_t L[NW];
+        load_L(s, L);
+        __syncwarp();
+        for (uint32_t i = lane; i < total; i += 32) {  // degree-one / degree-two triangle rules
+            const uint32_t v = s.cand()[i];
+            const uint32_t dv = s.degs16()[v];
+            uint32_t r[NW];
+            load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+            uint32_t n1 = kNone, hi = kNone;  // lowest and highest live neighbour
+#pragma unroll
+            for (int w = NW - 1; w >= 0; --w) {
+                const uint32_t x = r[w] & L[w];
+                n1 = x ? 32u * w + (__ffs(x) - 1) : n1;
+            }
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                const uint32_t x = r[w] & L[w];
+                hi = x ? 32u * w + (31u - __clz(x)) : hi;
+            }
+            const uint32_t n2 = dv == 2 ? hi : kNone;
+            if (dv == 1) {
+                const uint32_t du = s.degs16()[n1];
+                if (du > 1 || n1 < v) {
+                    atomicOr(&s.marks()[n1 >> 5], 1u << (n1 & 31u));
+                    marked = true;
+                }
+            } else if (n2 != kNone) {
+                const uint32_t d1 = s.degs16()[n1], d2 = s.degs16()[n2];
+                const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
+                if (!keep && ((s.adj[n2 * Rows<NW>::kStride + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
+                    atomicOr(&s.marks()[n1 >> 5], 1u << (n1 & 31u));
+                    atomicOr(&s.marks()[n2 >> 5], 1u << (n2 & 31u));
+                    marked = true;
+                }
+            }
+        }
+    }
+    s.stat.passes += 1;
+    if (__any_sync(0xffffffffu, marked)) {
+        __syncwarp();
+        return true;
+    }
+    uint32_t acc = 0, mx = 0;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const uint32_t d = s.D[j];
+        acc += (d & 0xFFFFu) + (d >> 16);
+        mx = max(mx, max(d & 0xFFFFu, d >> 16));
+    }
+    o.sum = __reduce_add_sync(0xffffffffu, acc);
+    o.maxd = __reduce_max_sync(0xffffffffu, mx);
+    uint32_t first = kNone;
+    if (o.maxd > 0) {
+#pragma unroll
+        for (int j = J - 1; j >= 0; --j) {
+            const uint32_t e = halves_zero(s.D[j] ^ (o.maxd * 0x00010001u));
+            if (e) first = 2u * (32u * j + lane) + ((__ffs(e) >> 4) - 1);
+        }
+    }
+    o.amax = __reduce_min_sync(0xffffffffu, first);
+    return false;
+}
+
+template <int NW>
+__device__ __forceinline__ bool dense_pass(DSU<NW> &s, uint32_t del, uint32_t bound, ScanOut &o)
+{
+    if constexpr (Rows<NW>::kHalf) return dense_pass_half(s, del, bound, o);
+    else return dense_pass_byte(s, del, bound, o);
 }
 
 // A node's settling: the pending set in s.marks() leaves L and the degrees are

@@ -118,6 +118,7 @@ struct Job {
     unsigned long long t0 = 0;
     bool aborted = false;
     bool wide = false;  // every graph may take the 20-word dense kernel
+    bool half = false;  // every graph may take the 16/32-word dense kernels (16-bit degrees)
     bool dev_input = false;  // the graphs came from the caller's device memory: checked by k_check_csr
     const Tune *tune = nullptr;  // a shape to try instead of the context's table (the tuner's candidates)
     Plan plan;
@@ -125,6 +126,13 @@ struct Job {
 
 // The largest graph of the wide dense kernel; it also needs every degree <= 254.
 constexpr uint32_t kWideMaxN = 640;
+
+// The largest graph of the dense kernels with 16-bit degrees (any degree).
+constexpr uint32_t kHalfMaxN = 1024;
+
+// True if a graph of n vertices takes a dense kernel with 16-bit degrees (when
+// the byte kernels cannot take it).
+inline bool half_ok(uint32_t n) { return n > 255 && n <= kHalfMaxN; }
 
 // True if a graph of n vertices (host row offsets) fits the wide dense kernel.
 inline bool wide_ok(uint32_t n, const uint32_t *row_ptr)
@@ -142,6 +150,7 @@ struct PlanOpts {
     bool wide = false;         // graphs of 256..640 vertices may take the wide dense kernel
     bool warp_gws = false;     // warp units with global-memory workspaces
     bool lanes = false;        // graphs <= 255 vertices take the lane kernel
+    bool half = false;         // graphs of 256..1024 vertices take the 16-bit-degree dense kernels
     bool team = false;         // CSR kernels walk rows with teams of lanes (average degree >= 4)
     const Tune *tune = nullptr; // the size class's tuned shape, if any
 };

@@ -75,8 +75,11 @@ __global__ void __launch_bounds__(NT, MinThreads / NT) k_search(Params P)
 template <int NW>
 struct DenseOcc {
     // 20-word graphs: three 256-thread CTAs' worth of registers (80 per thread),
-    // so that a server lane of them fits beside three 8-word CTAs per SM
-    static constexpr unsigned kThreads = NW >= 16 ? 768u : (NW >= 8 ? VC_DENSE8_THREADS : VC_DENSE4_THREADS);
+    // so that a server lane of them fits beside three 8-word CTAs per SM;
+    // 16- and 32-word graphs (16-bit degrees, rows and L in registers): two and
+    // one CTA per SM, as many as their staged adjacency leaves room for
+    static constexpr unsigned kThreads =
+        NW == 32 ? 256u : (NW == 16 ? 512u : (NW >= 16 ? 768u : (NW >= 8 ? VC_DENSE8_THREADS : VC_DENSE4_THREADS)));
     template <unsigned NT>
     static constexpr unsigned min_ctas() { return kThreads / NT < 32 ? kThreads / NT : 32; }  // 32 CTAs/SM at most
 };
@@ -274,13 +277,18 @@ static cudaError_t plan_dense(Ctx &c, Plan &pl, const Tune *t)
     const uint32_t budget = (uint32_t)c.smem_optin - 1024;
     uint32_t warps = (t && t->set) ? t->warps : VC_DENSE_WARPS;  // search units sharing one staged graph
     const uint32_t per_warp = (t && t->set) ? t->pool : 2;
+    // 32-word graphs (a 147 KB adjacency) step 8 -> 6 -> 4 warps, the others halve
     while (warps > 1 && dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(per_warp * warps, pl.stride) > budget)
-        warps >>= 1;
+        warps = (NW == 32 && warps == 8) ? 6 : (warps == 6 ? 4 : warps >> 1);
     pl.cta_slots = warps > 1 ? per_warp * warps : 0;
     uint32_t smem = dense_adj_bytes(NW) + warps * pl.su_bytes + cta_pool_bytes(pl.cta_slots, pl.stride);
     cudaError_t e;
     switch (warps) {
     case 8: e = plan_variant_fn<256>(c, pl, smem, k_dense<NW, 256>); break;
+    case 6:
+        if constexpr (NW == 32) e = plan_variant_fn<192>(c, pl, smem, k_dense<NW, 192>);
+        else e = cudaErrorInvalidConfiguration;
+        break;
     case 4: e = plan_variant_fn<128>(c, pl, smem, k_dense<NW, 128>); break;
     case 2: e = plan_variant_fn<64>(c, pl, smem, k_dense<NW, 64>); break;
     default: e = plan_variant_fn<32>(c, pl, smem, k_dense<NW, 32>); break;
@@ -339,6 +347,8 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
     if (nmax <= 128 && !c.force_sparse) return plan_dense<4>(c, pl, o.tune);
     if (nmax <= 255 && !c.force_sparse) return plan_dense<8>(c, pl, o.tune);
     if (nmax <= kWideMaxN && o.wide && !c.force_sparse) return plan_dense<20>(c, pl, o.tune);
+    if (nmax <= kHalfMaxN && o.half && !c.force_sparse)
+        return nmax <= 512 ? plan_dense<16>(c, pl, nullptr) : plan_dense<32>(c, pl, nullptr);
     const Tune *t = (o.tune && o.tune->set && !c.force_sparse) ? o.tune : nullptr;
     pl.np = np;
     pl.su_bytes = su_workspace_bytes(np);
@@ -417,6 +427,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     Plan pl;
     PlanOpts po;
     po.wide = job.wide;
+    po.half = job.half;
     po.team = sum_m2 >= 4 * sum_n && sum_n > 0;  // average degree 4 or more: rows walked by teams
     // Lane units (one thread per search unit, vc_lanes.cuh) are opt-in: they
     // execute half the instructions per tree node of warp units but, at 12
@@ -424,7 +435,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     // workload) and reach a quarter of the warp units' node rate.
     po.lanes = c.lanes_mode == 1;
     const Tune *tn = job.tune ? job.tune : &c.tune[tune_class(nmax, job.wide)];
-    po.tune = tn->set ? tn : nullptr;
+    po.tune = tn->set && !job.half ? tn : nullptr;  // the tuner's classes are measured on the other kernels
     if (make_plan(c, np, nmax, pl, po) != cudaSuccess) return VC_ERR_CUDA;
     const uint32_t stride = pl.stride;
     uint32_t q = 1024;
@@ -676,6 +687,7 @@ extern "C" vc_status vc_solve(const vc_csr *g, const vc_request *req, vc_result 
     job.desc.push_back(d);
     job.time_limit_s = req->time_limit_s;
     job.wide = !dev_in && wide_ok(g->n, g->row_ptr);
+    job.half = !job.wide && half_ok(g->n);
     job.dev_input = dev_in;
     vc_status s = run_job(*c, job, stream);
     if (s != VC_OK) { out->status = s; return s; }
@@ -755,20 +767,22 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         job.d_col = (const uint32_t *)c->col.p;
     }
     // One launch per kernel shape: dense bitsets (n <= 255), wide dense bitsets
-    // (n <= 640, every degree <= 254), warp search units (n <= kWarpMaxNP), CTA
-    // search units (larger); the shape is sized by the largest graph of its
-    // class, so small graphs never run in a large graph's workspace.  The row
-    // offsets are host arrays on both entry points.
+    // (n <= 640, every degree <= 254), dense bitsets with 16-bit degrees (n <=
+    // 1024), warp search units (n <= kWarpMaxNP), CTA search units (larger); the
+    // shape is sized by the largest graph of its class, so small graphs never
+    // run in a large graph's workspace.  The row offsets are host arrays on both
+    // entry points.
     auto klass = [&](uint32_t i) {
         const uint32_t n = a->n[i];
         if (n <= 255) return 0;
         if (wide_ok(n, a->row_ptr + a->row_off[i])) return 1;
-        return n <= kWarpMaxNP ? 2 : 3;
+        if (half_ok(n)) return 2;
+        return n <= kWarpMaxNP ? 3 : 4;
     };
     vc_status first = VC_OK;
     float total_kernel = 0;
     std::vector<uint32_t> members;
-    for (int cl = 0; cl < 4; ++cl) {
+    for (int cl = 0; cl < 5; ++cl) {
         members.clear();
         for (uint32_t i = 0; i < count; ++i)
             if (a->n[i] > 0 && klass(i) == cl) members.push_back(i);
@@ -777,6 +791,7 @@ vc_status vc_solve_batch_impl(const vc_csr_arena *a, const vc_request *reqs, vc_
         cj.d_rp = job.d_rp;
         cj.d_col = job.d_col;
         cj.wide = cl == 1;
+        cj.half = cl == 2;
         cj.dev_input = d_rp != nullptr;
         cj.desc.resize(members.size());
         double tl = 0;

@@ -116,19 +116,21 @@ VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
 }
 
 // Dense-bitset search unit (nw = 2, 4 or 8 words: graphs of at most 255
-// vertices; nw = 20: up to 640 vertices whose degrees are all at most 254):
-// per CTA adj[32*nw][dense_row_words(nw)] u32, then tri[nw] u32 (the vertices
-// that lie on a triangle of the staged graph); per warp
+// vertices; nw = 20: up to 640 vertices whose degrees are all at most 254;
+// nw = 16 and 32: up to 512 and 1024 vertices of any degree, with 16-bit
+// degrees): per CTA adj[32*nw][dense_row_words(nw)] u32, then tri[nw] u32 (the
+// vertices that lie on a triangle of the staged graph); per warp
 //   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 |
-//   cand[32*nw] u16 | degs[32*nw] u8
-// Row stride in words: 8-word rows are padded to 12 so that the 16-byte row
-// loads of eight consecutive lanes fall in distinct shared-memory banks
-// (20-word rows already do).
-VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw == 8 ? 12u : nw; }
+//   cand[32*nw] u16 | degs[32*nw] u8 (u16 with 16-bit degrees)
+// Row stride in words: 8-, 16- and 32-word rows are padded to 12, 20 and 36 so
+// that the 16-byte row loads of eight consecutive lanes fall in distinct
+// shared-memory banks (20-word rows already do).
+VC_HD inline bool dense_half(uint32_t nw) { return nw == 16 || nw == 32; }
+VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw == 8 ? 12u : (dense_half(nw) ? nw + 4u : nw); }
 VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw) + 128u; }
 VC_HD inline uint32_t dense_workspace_bytes(uint32_t nw)
 {
-    uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 2u * 32u * nw + 32u * nw;
+    uint32_t b = 4u * (32u * nw + 3u * nw) + 2u * 32u * nw + 2u * 32u * nw + (dense_half(nw) ? 2u : 1u) * 32u * nw;
     return (b + 15u) & ~15u;
 }
 

@@ -269,23 +269,62 @@ def test_wide_dense_kernel_batched_and_plain():
         _check_pvc(g, vcgpu.solve(g, "pvc", k=opt, time_limit=TL), opt, 1)
 
 
-def test_wide_range_with_a_high_degree_vertex_takes_csr():
-    """A 300-vertex graph with a vertex of degree 280 does not fit byte degrees:
-    it runs on the CSR kernel and stays exact."""
-    rng = np.random.default_rng(7)
-    n = 300
-    base = W.gnp(n, 2.5 / (n - 1), 99)
-    e = [(u, v) for u in range(n) for v in base.col[base.row_ptr[u]:base.row_ptr[u + 1]] if u < v]
-    hub = set(int(x) for x in rng.choice(np.arange(1, n), 280, replace=False))
-    e = list({(min(u, v), max(u, v)) for u, v in e + [(0, h) for h in hub]})
-    g = W.from_edges(n, np.asarray(e, dtype=np.int64), "hub300")
-    assert int(np.diff(g.row_ptr).max()) > 254
-    st, opt, _, _ = O.mvc(g, node_limit=2_000_000)
-    assert st == O.OK
-    r = vcgpu.solve(g, "mvc", time_limit=TL)
+def _hub_graphs():
+    """Graphs of 256..1024 vertices with one to three hubs of degree above 254 on
+    a sparse G(n, p) base: the range of the dense kernels with 16-bit degrees,
+    with the oracle's optima."""
+    rng = np.random.default_rng(2024)
+    out = []
+    for n, hubs in ((300, 1), (420, 2), (512, 1), (600, 2), (800, 3), (1000, 2), (1024, 1)):
+        base = W.gnp(n, 3.0 / (n - 1), int(rng.integers(1 << 30)))
+        e = [(u, int(v)) for u in range(n) for v in base.col[base.row_ptr[u]:base.row_ptr[u + 1]] if u < v]
+        for h in range(hubs):
+            k = min(n - hubs, max(260, int(n * rng.uniform(0.6, 0.9))))
+            e += [(h, int(x)) for x in rng.choice(np.arange(hubs, n), k, replace=False)]
+        e = list({(min(u, v), max(u, v)) for u, v in e})
+        g = W.from_edges(n, np.asarray(e, dtype=np.int64), f"hub{n}x{hubs}")
+        assert int(np.diff(g.row_ptr).max()) > 254
+        st, opt, _, _ = O.mvc(g, node_limit=2_000_000)
+        if st == O.OK:
+            out.append((g, opt))
+    return out
+
+
+def test_half_dense_kernels_batched_and_plain():
+    """Degrees above a byte (up to 1024 vertices) run on the dense kernels with
+    16-bit degrees (16-word rows up to 512 vertices, 32-word rows above),
+    batched and one at a time, with the oracle's optima and decisions."""
+    items = _hub_graphs()
+    assert len(items) >= 6
+    graphs = [g for g, _ in items]
+    st, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=TL)
+    assert st == vcgpu.VC_OK
     _, shape = vcgpu.debug_stats()
-    assert int(shape[4]) >> 31 == 0, shape  # CSR plan
-    _check_mvc(g, r, opt)
+    assert int(shape[4]) >> 31 == 1 and (int(shape[4]) & 0x7FFFFFFF) == 1024, shape  # the 32-word dense plan ran
+    for (g, opt), r in zip(items, sols):
+        _check_mvc(g, r, opt)
+    for g, opt in items:
+        r = vcgpu.solve(g, "mvc", time_limit=TL)
+        _, shape = vcgpu.debug_stats()
+        assert int(shape[4]) >> 31 == 1 and (int(shape[4]) & 0x7FFFFFFF) == (512 if g.n <= 512 else 1024), shape
+        _check_mvc(g, r, opt)
+        _check_pvc(g, vcgpu.solve(g, "pvc", k=opt - 1, time_limit=TL), opt - 1, 0)
+        _check_pvc(g, vcgpu.solve(g, "pvc", k=opt, time_limit=TL), opt, 1)
+
+
+def test_half_dense_range_on_the_csr_kernel():
+    """The same graphs forced onto the CSR kernel (rows walked by teams of
+    lanes where the average degree allows) stay exact."""
+    items = _hub_graphs()[:4]
+    vcgpu.debug_stats(2)  # force the CSR kernel
+    try:
+        st, sols = vcgpu.solve_batch(W.pack([g for g, _ in items]), "mvc", time_limit=TL)
+        _, shape = vcgpu.debug_stats()
+    finally:
+        vcgpu.debug_stats(0)
+    assert st == vcgpu.VC_OK and int(shape[4]) >> 31 == 0, shape
+    for (g, opt), r in zip(items, sols):
+        _check_mvc(g, r, opt)
 
 
 def test_batch_pvc_vs_golden():
