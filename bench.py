@@ -30,9 +30,11 @@ set); `--set full` runs all 4096.
 
 `--impl reference` runs only the reference's CPU solver over the CPU sample
 (rank 0 only under torchrun).  `--workload stream` runs the served configuration
-alone for longer; `--workload ub` the upper-bound heuristics; `--workload profile`
-is the torch-free case for profiler captures: the first --count graphs of the
-step's set in one vc_solve_batch call, --reps times.
+alone for longer; `--workload ub` the upper-bound heuristics; `--workload files`
+the reference's own graph files (staged by `make -C oracle graphs`) through
+vc_solve beside the reference's own CUDA program on the same files; `--workload
+profile` is the torch-free case for profiler captures: the first --count graphs
+of the step's set in one vc_solve_batch call, --reps times.
 
 Multi-GPU: `--gpus N` starts N ranks under torch.distributed.run when it is not
 already running under it.  The pinned set is split across the ranks by
@@ -74,7 +76,11 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub", "profile"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub", "profile", "files"])
+    ap.add_argument("--files", default="",
+                    help="--workload files: comma-separated reference graph files (default: the 1-based ones)")
+    ap.add_argument("--file-time-limit", type=float, default=30.0,
+                    help="--workload files: seconds per solve, for this library and the reference's program alike")
     ap.add_argument("--count", type=int, default=128)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--case", default="batch", choices=["batch", "csr-batch", "powergrid", "file"])
@@ -668,6 +674,78 @@ def stream_arm(args, world, rank):
     print(json.dumps(line))
 
 
+# The reference's graph files its loader reads as they are (1-based ids;
+# auxFunctions.cpp:150-154 shifts every id down by one, so the 0-based
+# formated_* and lastfm files are not valid input to it).
+REF_FILES_1BASED = ["cop_hat300-1.txt", "cop_hat300-2.txt", "cop_hat300-3.txt", "cop_hat500-1.txt", "cop_hat500-2.txt",
+                    "cop_hat500-3.txt", "cop_hat700-1.txt", "cop_hat700-2.txt", "cop_hat1000-1.txt",
+                    "cop_hat1000-2.txt", "Power-Grid.txt", "Sister-Cities.txt", "vc-exact_009.txt", "vc-exact_023.txt"]
+# Files the reference's program is not run on: its stacks take (UB + 1) * n * 4
+# bytes per block (stack.cuh:39, unchecked cudaMalloc), about 1.8 GB per block
+# and hundreds of GB in all for these, so its kernel would run on a failed
+# allocation.
+REF_CUDA_NOT_RUN = {"vc-exact_009.txt": "stack allocation of (UB+1)*n*4 bytes per block (~3.3 GB) fails unchecked",
+                    "vc-exact_023.txt": "stack allocation of (UB+1)*n*4 bytes per block (~1.8 GB) fails unchecked"}
+
+
+def files_arm(args, world, rank):
+    """The reference's graph files (test/test_graphs, known optima from
+    test/runGraphs.py:8-30): this library's plain vc_solve (host buffers, no
+    upper bound given) and the reference's own CUDA program (oracle/_ref/cuda/
+    output: hybrid MVC kernel, default sizing, its CPU upper bounds first), each
+    with --file-time-limit seconds per file.  Reports per file the kernel time,
+    the call's time and whether the answer equals the known optimum."""
+    if rank != 0:
+        return
+    import gzip
+    import shutil
+    import vcgpu
+    known = json.load(open(os.path.join(REPO, "tests", "golden", "known_answers.json")))["mvc"]
+    names = [f for f in args.files.split(",") if f] or REF_FILES_1BASED
+    tl = args.file_time_limit
+    rows = []
+    for name in names:
+        src = os.path.join(REPO, "oracle", "_ref", "graphs", name + ".gz")
+        if not os.path.exists(src):
+            rows.append({"file": name, "missing": "stage with `make -C oracle graphs`"})
+            continue
+        zero = name.startswith("formated_") or name.startswith("lastfm")
+        g = W.read_reference_file(src, one_based=not zero)
+        r = vcgpu.solve(g, "mvc", time_limit=tl)
+        r = vcgpu.solve(g, "mvc", time_limit=tl) if r.status == vcgpu.VC_OK else r  # warm: time the second call
+        ok = r.status == vcgpu.VC_OK and r.size == known[name] and W.is_cover(g, r.cover)
+        ours = {"status": vcgpu.STATUS_NAMES.get(r.status, r.status), "size": r.size, "correct": bool(ok),
+                "kernel_ms": round(r.kernel_ms, 2), "call_ms": round(r.total_ms, 2), "tree_nodes": int(r.tree_nodes)}
+        ref = {"unavailable": "oracle/_ref/cuda/output not built"}
+        if name in REF_CUDA_NOT_RUN:
+            ref = {"not_run": REF_CUDA_NOT_RUN[name]}
+        elif os.path.exists(REF_CUDA) and not zero:
+            with tempfile.TemporaryDirectory() as td:
+                os.makedirs(os.path.join(td, "Results"))
+                path = os.path.join(td, name)
+                with gzip.open(src, "rb") as fi, open(path, "wb") as fo:
+                    shutil.copyfileobj(fi, fo)
+                t0 = time.perf_counter()
+                try:
+                    p = subprocess.run([REF_CUDA, "-f", path, "-o", "files"], cwd=td, capture_output=True, text=True,
+                                       timeout=tl + 30)
+                    wall = time.perf_counter() - t0
+                    row = open(os.path.join(td, "Results", "Results.csv")).read().strip().splitlines()[-1].split(",")
+                    size = int(row[18])
+                    ref = {"status": "ok" if p.returncode == 0 else f"exit {p.returncode}", "size": size,
+                           "correct": p.returncode == 0 and size == known[name], "kernel_ms": float(row[21]),
+                           "process_s": round(wall, 2), "cpu_upper_bounds": [int(row[14]), int(row[16])]}
+                except subprocess.TimeoutExpired:
+                    ref = {"status": "timeout", "process_s": tl + 30}
+                except (OSError, IndexError, ValueError) as e:
+                    ref = {"status": "error", "error": repr(e)[:120]}
+        rows.append({"file": name, "n": g.n, "m": g.m, "known_opt": known[name], "ours": ours, "reference_cuda": ref})
+    line = {"metric": "reference graph files: kernel ms per file, this library vs the reference's CUDA program",
+            "unit": "ms", "higher_is_better": False, "n_gpus": 1, "data": "the reference's test/test_graphs files",
+            "time_limit_s": tl, "files": rows}
+    print(json.dumps(line))
+
+
 def ub_arm(args, world, rank):
     """The reference's upper-bound heuristics on the GPU (vc_remove_max_ub /
     vc_remove_edge_ub): Chung-Lu n=100000 (one graph) and the 4096 batched
@@ -751,6 +829,8 @@ def main():
             stream_arm(args, world, rank)
         elif args.workload == "ub":
             ub_arm(args, world, rank)
+        elif args.workload == "files":
+            files_arm(args, world, rank)
         else:
             our_arm(args, world, rank, local, pg)
     finally:

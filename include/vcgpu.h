@@ -148,7 +148,7 @@ vc_status vc_remove_edge_ub(const vc_csr_arena *arena, uint32_t r, int32_t devic
 /* The autotuner (replaces the reference's fixed launch-sizing rule,
  * setBlockDimAndUseGlobalMemoryAutoWorkListSize, src/auxFunctions.cpp:469-578):
  * for each size class of graphs (dense n <= 64, <= 128, <= 255; wide dense
- * n <= 640; CSR n <= 1024; CSR larger) it times candidate launch shapes -- warp
+ * n <= 640; 16-bit dense n <= 1024; CSR larger) it times candidate launch shapes -- warp
  * or CTA search units, warps per CTA, CTA pool slots (the shared-memory stack
  * of donated subtrees) per warp, the global-ring donation threshold and the
  * donation order -- on seeded calibration graphs of the class for slice_s

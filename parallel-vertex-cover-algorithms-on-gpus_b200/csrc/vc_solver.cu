@@ -348,7 +348,7 @@ cudaError_t make_plan(Ctx &c, uint32_t np, uint32_t nmax, Plan &pl, const PlanOp
     if (nmax <= 255 && !c.force_sparse) return plan_dense<8>(c, pl, o.tune);
     if (nmax <= kWideMaxN && o.wide && !c.force_sparse) return plan_dense<20>(c, pl, o.tune);
     if (nmax <= kHalfMaxN && o.half && !c.force_sparse)
-        return nmax <= 512 ? plan_dense<16>(c, pl, nullptr) : plan_dense<32>(c, pl, nullptr);
+        return nmax <= 512 ? plan_dense<16>(c, pl, o.tune) : plan_dense<32>(c, pl, o.tune);
     const Tune *t = (o.tune && o.tune->set && !c.force_sparse) ? o.tune : nullptr;
     pl.np = np;
     pl.su_bytes = su_workspace_bytes(np);
@@ -435,7 +435,7 @@ vc_status run_job(Ctx &c, Job &job, cudaStream_t stream)
     // workload) and reach a quarter of the warp units' node rate.
     po.lanes = c.lanes_mode == 1;
     const Tune *tn = job.tune ? job.tune : &c.tune[tune_class(nmax, job.wide)];
-    po.tune = tn->set && !job.half ? tn : nullptr;  // the tuner's classes are measured on the other kernels
+    po.tune = tn->set ? tn : nullptr;
     if (make_plan(c, np, nmax, pl, po) != cudaSuccess) return VC_ERR_CUDA;
     const uint32_t stride = pl.stride;
     uint32_t q = 1024;

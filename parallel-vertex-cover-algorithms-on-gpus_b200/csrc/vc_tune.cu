@@ -7,9 +7,11 @@
 // global-memory variant when none does, and a worklist size halved until it
 // fits).  Here the library's built-in rules pick the kernel by graph size; the
 // tuner measures, per size class, the alternatives those rules leave open:
-//   * warp search units or one 512-thread CTA per search unit (CSR classes),
-//   * warps per CTA (2, 4, 8) -- how many search units share one staged graph
-//     and one CTA pool,
+//   * warp search units or one 512-thread CTA per search unit (the CSR class,
+//     above 1024 vertices),
+//   * warps per CTA (2, 4, 8; 6 stands for 8 where a 1024-vertex graph's
+//     adjacency leaves no room) -- how many search units share one staged graph
+//     and one CTA pool (the dense classes up to 1024 vertices),
 //   * CTA pool slots per warp (1, 2, 4) -- the depth of the shared-memory stack
 //     of donated subtrees,
 //   * the ring threshold: work goes to the global ring while idle CTAs minus
@@ -103,7 +105,7 @@ const ClassSpec kSpec[kTuneClasses] = {
 // Runs the class's calibration batch with one candidate shape for `slice_s`
 // seconds (the launch's time limit; each graph also has a node limit) and
 // returns its tree nodes per second.
-double measure(Ctx &c, const std::vector<CalGraph> &gs, const Tune &cand, double slice_s, bool wide)
+double measure(Ctx &c, const std::vector<CalGraph> &gs, const Tune &cand, double slice_s, bool wide, bool half)
 {
     uint64_t rows = 0, cols = 0;
     for (const auto &g : gs) { rows += g.n + 1; cols += g.col.size(); }
@@ -134,6 +136,7 @@ double measure(Ctx &c, const std::vector<CalGraph> &gs, const Tune &cand, double
     job.d_col = (const uint32_t *)c.col.p;
     job.time_limit_s = slice_s;
     job.wide = wide;
+    job.half = half;
     job.tune = &cand;
     if (run_job(c, job, c.stream) != VC_OK) return -1;
     uint64_t nodes = 0;
@@ -188,9 +191,9 @@ extern "C" vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table
             const double d = sp.d_lo + (sp.d_hi - sp.d_lo) * r.uniform();
             gs.push_back(gnm(r, n, d));
         }
-        const bool wide = k == 3;
+        const bool wide = k == 3, half = k == 4;  // the kernels the class's graphs take
         std::vector<Tune> cands;
-        if (k <= 3) {
+        if (k <= 4) {
             for (uint32_t w : {2u, 4u, 8u})
                 for (uint32_t p : {1u, 2u, 4u}) cands.push_back(Tune{1, 0, w, p, 0, 0});
         } else {
@@ -200,19 +203,19 @@ extern "C" vc_status vc_autotune(int32_t device, double slice_s, uint32_t *table
         Tune best{};
         double best_rate = -1;
         for (Tune &t : cands) {
-            const double rate = measure(*c, gs, t, slice_s, wide);
+            const double rate = measure(*c, gs, t, slice_s, wide, half);
             if (rate > best_rate) { best_rate = rate; best = t; }
         }
         for (int32_t bias : {-64, -16, 4, 32}) {  // then the ring threshold, with the best shape
             Tune t = best;
             t.ring_bias = bias;
-            const double rate = measure(*c, gs, t, slice_s, wide);
+            const double rate = measure(*c, gs, t, slice_s, wide, half);
             if (rate > best_rate) { best_rate = rate; best = t; }
         }
         {  // then the donation order
             Tune t = best;
             t.ring_first = 1;
-            const double rate = measure(*c, gs, t, slice_s, wide);
+            const double rate = measure(*c, gs, t, slice_s, wide, half);
             if (rate > best_rate) { best_rate = rate; best = t; }
         }
         if (best_rate <= 0) return VC_ERR_CUDA;

@@ -286,7 +286,7 @@ def kernel_launches() -> int:
     return int(lib().vc_kernel_launches())
 
 
-TUNE_CLASSES = ["dense n<=64", "dense n<=128", "dense n<=255", "wide dense n<=640", "csr n<=1024", "csr n>1024"]
+TUNE_CLASSES = ["dense n<=64", "dense n<=128", "dense n<=255", "wide dense n<=640", "16-bit dense n<=1024", "csr n>1024"]
 
 
 TUNE_WORDS = 7  # per class

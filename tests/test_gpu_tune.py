@@ -29,7 +29,7 @@ def test_autotune_installs_valid_shapes_and_answers_stay_exact():
         recs = _golden(500_000, 120)
         graphs = [W.batch_instance(r["i"]) for r in recs]
         rng = np.random.default_rng(5)
-        for n in (700, 1500):  # the two CSR classes
+        for n in (700, 1500):  # the 16-bit dense class and the CSR class
             graphs.append(W.gnp(n, 2.5 / (n - 1), int(rng.integers(1 << 30))))
         opts = [r["opt"] for r in recs] + [vcgpu.solve(g, "mvc", time_limit=60).size for g in graphs[len(recs):]]
         _, sols = vcgpu.solve_batch(W.pack(graphs), "mvc", time_limit=60.0)
