@@ -173,27 +173,71 @@ __device__ __forceinline__ void live_nibbles(DSU<NW> &s)
     }
 }
 
-// Degrees from scratch: one vertex per lane into the byte staging array, then
-// each lane picks up its words.
+// Degrees from scratch into the staging array, then each lane picks up its
+// words.  With 4-word row chunks (NW = 8, 16, 20, 32) only the live vertices
+// are counted -- listed by a prefix sum over the words of L, then one per lane
+// -- and only over the chunks of L that hold a live vertex; the staging array
+// is zeroed first, so removed and padding vertices read 0.  Deep in a dense
+// graph's tree most vertices are gone, and this is most of a node's work.
 template <int NW>
 __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
 {
     const unsigned lane = lane_id();
-    const int kmax = (int)s.nw;
     uint32_t L[NW];
     load_L(s, L);
-#pragma unroll 1
-    for (int k = 0; k < kmax; ++k) {
-        const uint32_t v = lane + 32u * k;
-        uint32_t c = 0;
-        if (v < s.n && ((s.lsm()[k] >> lane) & 1u)) {
-            uint32_t r[NW];
-            load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+    if constexpr (NW % 4 == 0) {
+        constexpr int C = NW / 4;
+        uint32_t nzc = 0;  // chunks of L with a live vertex (the same in every lane)
 #pragma unroll
-            for (int w = 0; w < NW; ++w) c += __popc(r[w] & L[w]);
+        for (int c = 0; c < C; ++c) nzc |= (uint32_t)((L[4 * c] | L[4 * c + 1] | L[4 * c + 2] | L[4 * c + 3]) != 0u) << c;
+        uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs());
+        constexpr uint32_t kStageWords = 32u * NW / Rows<NW>::kPer;
+        for (uint32_t i = lane; i < kStageWords; i += 32) d32[i] = 0u;
+        const uint32_t x = lane < (uint32_t)NW ? s.lsm()[lane] : 0u;
+        const uint32_t cnt = __popc(x);
+        uint32_t off = cnt;  // inclusive prefix over the words of L
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, off, d);
+            if (lane >= (unsigned)d) off += t;
         }
-        if constexpr (Rows<NW>::kHalf) s.degs16()[v] = (uint16_t)c;
-        else s.degs()[v] = (uint8_t)c;
+        const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
+        uint16_t *list = s.cand();  // free while the degrees are recounted
+        uint32_t pos = off - cnt, m = x;
+        while (m) {
+            list[pos++] = (uint16_t)(32u * lane + (__ffs(m) - 1));
+            m &= m - 1;
+        }
+        __syncwarp();
+        for (uint32_t i = lane; i < total; i += 32) {
+            const uint32_t v = list[i];
+            const uint4 *row = reinterpret_cast<const uint4 *>(s.adj + v * Rows<NW>::kStride);
+            uint32_t c = 0;
+#pragma unroll
+            for (int k = 0; k < C; ++k) {
+                if ((nzc >> k) & 1u) {
+                    const uint4 r = row[k];
+                    c += __popc(r.x & L[4 * k]) + __popc(r.y & L[4 * k + 1]) + __popc(r.z & L[4 * k + 2]) +
+                         __popc(r.w & L[4 * k + 3]);
+                }
+            }
+            if constexpr (Rows<NW>::kHalf) s.degs16()[v] = (uint16_t)c;
+            else s.degs()[v] = (uint8_t)c;
+        }
+    } else {  // 2- and 4-word graphs: one vertex per lane
+        const int kmax = (int)s.nw;
+#pragma unroll 1
+        for (int k = 0; k < kmax; ++k) {
+            const uint32_t v = lane + 32u * k;
+            uint32_t c = 0;
+            if (v < s.n && ((s.lsm()[k] >> lane) & 1u)) {
+                uint32_t r[NW];
+                load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+#pragma unroll
+                for (int w = 0; w < NW; ++w) c += __popc(r[w] & L[w]);
+            }
+            s.degs()[v] = (uint8_t)c;
+        }
     }
     __syncwarp();
     const uint32_t *d32 = reinterpret_cast<const uint32_t *>(s.degs());
