@@ -38,7 +38,13 @@ namespace vcg {
 template <int NW>
 struct Rows {
     static constexpr bool kHalf = NW == 16 || NW == 32;  // 16-bit degrees (dense_half)
-    static constexpr int kStride = NW == 8 ? 12 : (kHalf ? NW + 4 : NW);  // dense_row_words
+    static constexpr int kStride = NW == 8 ? 12 : (NW == 16 ? 20 : NW);  // dense_row_words
+    static constexpr bool kSwz = NW == 32;  // 16-byte chunks of a row XOR-swizzled by the row's low 3 bits
+    // Index of word w of row v.
+    static __device__ __forceinline__ uint32_t at(uint32_t v, uint32_t w)
+    {
+        return v * kStride + (kSwz ? ((((w >> 2) ^ (v & 7u)) << 2) | (w & 3u)) : w);
+    }
     static constexpr int kPer = kHalf ? 2 : 4;                             // degrees per word
     static constexpr int kJ = kHalf ? NW / 2 : (NW >= 8 ? NW / 4 : 1);     // degree words per lane
     // bits of a lane's candidate count (at most kPer * kJ)
@@ -151,6 +157,22 @@ __device__ __forceinline__ void load_row(const uint32_t *row, uint32_t (&r)[NW],
     }
 }
 
+// Row v of the adjacency (logical word order) into registers.
+template <int NW>
+__device__ __forceinline__ void load_row_at(const uint32_t *adj, uint32_t v, uint32_t (&r)[NW])
+{
+    if constexpr (Rows<NW>::kSwz) {
+        const uint32_t sw = v & 7u;
+#pragma unroll
+        for (int c = 0; c < NW / 4; ++c) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(adj + v * Rows<NW>::kStride + 4u * ((uint32_t)c ^ sw));
+            r[4 * c] = q.x; r[4 * c + 1] = q.y; r[4 * c + 2] = q.z; r[4 * c + 3] = q.w;
+        }
+    } else {
+        load_row<NW>(adj + v * Rows<NW>::kStride, r, NW);
+    }
+}
+
 // All NW words of L into registers.
 template <int NW>
 __device__ __forceinline__ void load_L(const DSU<NW> &s, uint32_t (&L)[NW])
@@ -212,11 +234,12 @@ __device__ __forceinline__ void dense_degrees(DSU<NW> &s)
         for (uint32_t i = lane; i < total; i += 32) {
             const uint32_t v = list[i];
             const uint4 *row = reinterpret_cast<const uint4 *>(s.adj + v * Rows<NW>::kStride);
+            const uint32_t sw = Rows<NW>::kSwz ? (v & 7u) : 0u;
             uint32_t c = 0;
 #pragma unroll
             for (int k = 0; k < C; ++k) {
                 if ((nzc >> k) & 1u) {
-                    const uint4 r = row[k];
+                    const uint4 r = row[(uint32_t)k ^ sw];
                     c += __popc(r.x & L[4 * k]) + __popc(r.y & L[4 * k + 1]) + __popc(r.z & L[4 * k + 2]) +
                          __popc(r.w & L[4 * k + 3]);
                 }
@@ -305,7 +328,7 @@ __device__ __forceinline__ void dense_apply_half(DSU<NW> &s)
     {
         // word 2j + lane/16 of a row holds the bits of this lane's vertices 2q, 2q+1
         const uint32_t sh = 2u * (lane & 15u);
-        const uint32_t *rows = s.adj + (lane >> 4);
+        const uint32_t hl = lane >> 4;
         const uint32_t mw = lane < s.nw ? s.marks()[lane] : 0u;
         uint32_t wm = __ballot_sync(0xffffffffu, mw != 0u);
         uint32_t acc[J];
@@ -318,9 +341,8 @@ __device__ __forceinline__ void dense_apply_half(DSU<NW> &s)
             while (m) {
                 const uint32_t u = 32u * w + (__ffs(m) - 1);
                 m &= m - 1;
-                const uint32_t *r = rows + u * Rows<NW>::kStride;
 #pragma unroll
-                for (int j = 0; j < J; ++j) acc[j] += spread2((r[2 * j] >> sh) & s.Ln[j]);
+                for (int j = 0; j < J; ++j) acc[j] += spread2((s.adj[Rows<NW>::at(u, 2u * j + hl)] >> sh) & s.Ln[j]);
             }
         }
 #pragma unroll
@@ -551,7 +573,7 @@ __device__ __forceinline__ bool dense_pass_half(DSU<NW> &s, uint32_t del, uint32
             const uint32_t v = s.cand()[i];
             const uint32_t dv = s.degs16()[v];
             uint32_t r[NW];
-            load_row<NW>(s.adj + v * Rows<NW>::kStride, r, NW);
+            load_row_at<NW>(s.adj, v, r);
             uint32_t n1 = kNone, hi = kNone;  // lowest and highest live neighbour
 #pragma unroll
             for (int w = NW - 1; w >= 0; --w) {
@@ -573,7 +595,7 @@ __device__ __forceinline__ bool dense_pass_half(DSU<NW> &s, uint32_t del, uint32
             } else if (n2 != kNone) {
                 const uint32_t d1 = s.degs16()[n1], d2 = s.degs16()[n2];
                 const bool keep = d1 == 1 || d2 == 1 || (d1 == 2 && n1 < v) || (d2 == 2 && n2 < v);
-                if (!keep && ((s.adj[n2 * Rows<NW>::kStride + (n1 >> 5)] >> (n1 & 31u)) & 1u)) {
+                if (!keep && ((s.adj[Rows<NW>::at(n2, n1 >> 5)] >> (n1 & 31u)) & 1u)) {
                     atomicOr(&s.marks()[n1 >> 5], 1u << (n1 & 31u));
                     atomicOr(&s.marks()[n2 >> 5], 1u << (n2 & 31u));
                     marked = true;
@@ -706,7 +728,7 @@ __device__ __forceinline__ void donation_bits(DSU<NW> &s)
         atomicOr(&s.bits()[u >> 5], 1u << (u & 31u));
     }
     __syncwarp();
-    if (lane < NW) s.bits()[lane] &= ~s.adj[v * Rows<NW>::kStride + lane];
+    if (lane < NW) s.bits()[lane] &= ~s.adj[Rows<NW>::at(v, lane)];
     __syncwarp();
 }
 
@@ -737,12 +759,11 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
     // drops a graph it flags.
     const uint32_t m2 = d.m2 != kNone ? min(__ldcg(&rp[d.n]), d.m2) : __ldcg(&rp[d.n]);
     for (uint32_t v = lane; v < d.n; v += 32) {  // row v belongs to lane v % 32
-        uint32_t *row = adj + v * Rows<NW>::kStride;
         const uint32_t e1 = min(__ldcg(&rp[v + 1]), m2);
         for (uint32_t e = __ldcg(&rp[v]); e < e1; ++e) {
             const uint32_t u = __ldcg(&cl[e]);
             if (u >= d.n || u == v) continue;
-            row[u >> 5] |= 1u << (u & 31u);
+            adj[Rows<NW>::at(v, u >> 5)] |= 1u << (u & 31u);
         }
     }
     __syncwarp();
@@ -751,17 +772,17 @@ __device__ __forceinline__ void stage_graph(uint32_t *adj, const Params &P, uint
     // passes look at degree-2 vertices in tri only.
     for (uint32_t v = lane; v < d.n; v += 32) {
         uint32_t r[NW];
-        load_row<NW>(adj + v * Rows<NW>::kStride, r, NW);
+        load_row_at<NW>(adj, v, r);
         bool t = false;
 #pragma unroll 1
         for (uint32_t w = 0; w < (uint32_t)NW && !t; ++w) {
-            uint32_t x = adj[v * Rows<NW>::kStride + w];
+            uint32_t x = adj[Rows<NW>::at(v, w)];
             while (x && !t) {
                 const uint32_t u = 32u * w + (__ffs(x) - 1);
                 x &= x - 1;
                 uint32_t c = 0;
 #pragma unroll
-                for (int k = 0; k < NW; ++k) c |= adj[u * Rows<NW>::kStride + k] & r[k];
+                for (int k = 0; k < NW; ++k) c |= adj[Rows<NW>::at(u, k)] & r[k];
                 t = c != 0u;
             }
         }
@@ -956,7 +977,7 @@ __device__ void su_main_dense(const Params &P, uint8_t *ws, uint32_t *adj, CtaPo
                 const uint32_t f = s.frames()[s.fr_top];
                 const uint32_t v = f & 0xffffu;
                 dense_restore(s, f >> 16);
-                if (lane < NW) s.marks()[lane] = s.adj[v * Rows<NW>::kStride + lane] & s.lsm()[lane];
+                if (lane < NW) s.marks()[lane] = s.adj[Rows<NW>::at(v, lane)] & s.lsm()[lane];
                 __syncwarp();
                 s.pending = kPendRecount;  // take N(v), then recount
                 have = true;

@@ -122,11 +122,13 @@ VC_HD inline uint32_t su_workspace_bytes(uint32_t np)
 // vertices that lie on a triangle of the staged graph); per warp
 //   frames[32*nw] u32 | marks[nw] | bits[nw] | lsm[nw] | trail[32*nw] u16 |
 //   cand[32*nw] u16 | degs[32*nw] u8 (u16 with 16-bit degrees)
-// Row stride in words: 8-, 16- and 32-word rows are padded to 12, 20 and 36 so
-// that the 16-byte row loads of eight consecutive lanes fall in distinct
-// shared-memory banks (20-word rows already do).
+// Row stride in words: 8- and 16-word rows are padded to 12 and 20 so that the
+// 16-byte row loads of eight consecutive lanes fall in distinct shared-memory
+// banks (20-word rows already do); 32-word rows are not padded (a 1024-vertex
+// adjacency is 128 KB) but their eight 16-byte chunks are stored XOR-swizzled
+// by the row's low three bits, which spreads the same loads as well.
 VC_HD inline bool dense_half(uint32_t nw) { return nw == 16 || nw == 32; }
-VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw == 8 ? 12u : (dense_half(nw) ? nw + 4u : nw); }
+VC_HD inline uint32_t dense_row_words(uint32_t nw) { return nw == 8 ? 12u : (nw == 16 ? 20u : nw); }
 VC_HD inline uint32_t dense_adj_bytes(uint32_t nw) { return 4u * 32u * nw * dense_row_words(nw) + 128u; }
 VC_HD inline uint32_t dense_workspace_bytes(uint32_t nw)
 {
