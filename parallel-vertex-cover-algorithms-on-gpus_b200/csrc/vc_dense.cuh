@@ -430,13 +430,16 @@ __device__ __forceinline__ bool dense_pass_byte(DSU<NW> &s, uint32_t del, uint32
         ctot += __popc(cn[j]);
     }
     // compact the degree-1/2 candidates (at most 4J per lane) into s.cand()
+    // (one vote first: many passes have none)
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t pre = 0, total = 0;
+    if (__any_sync(0xffffffffu, ctot != 0u)) {
 #pragma unroll
-    for (int b = 0; b < Rows<NW>::kCandBits; ++b) {
-        const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
-        pre += __popc(bal & lt) << b;
-        total += __popc(bal) << b;
+        for (int b = 0; b < Rows<NW>::kCandBits; ++b) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
+            pre += __popc(bal & lt) << b;
+            total += __popc(bal) << b;
+        }
     }
     if (total) {
         uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs());
@@ -547,11 +550,13 @@ __device__ __forceinline__ bool dense_pass_half(DSU<NW> &s, uint32_t del, uint32
     }
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t pre = 0, total = 0;
+    if (__any_sync(0xffffffffu, ctot != 0u)) {
 #pragma unroll
-    for (int b = 0; b < Rows<NW>::kCandBits; ++b) {
-        const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
-        pre += __popc(bal & lt) << b;
-        total += __popc(bal) << b;
+        for (int b = 0; b < Rows<NW>::kCandBits; ++b) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, (ctot >> b) & 1u);
+            pre += __popc(bal & lt) << b;
+            total += __popc(bal) << b;
+        }
     }
     if (total) {
         uint32_t *d32 = reinterpret_cast<uint32_t *>(s.degs16());
