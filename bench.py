@@ -26,6 +26,9 @@ set); `--set full` runs all 4096.
           call and in one batched call
   config.reference_cuda: the reference's own CUDA program (oracle/_ref/cuda/output,
           built for sm_100a by oracle/Makefile), one process per graph
+  config.reference_files: the same program and vc_solve on six of the
+          reference's own graph files (--ref-files), answers checked against
+          its known optima
   config.served: a short served stream through vc_server
 
 `--impl reference` runs only the reference's CPU solver over the CPU sample
@@ -93,6 +96,10 @@ def parse(argv=None):
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--ref-step-s", type=float, default=15.0)
     ap.add_argument("--refcuda-graphs", type=int, default=16)
+    ap.add_argument("--ref-files", default="cop_hat300-1.txt,cop_hat500-1.txt,cop_hat500-2.txt,cop_hat700-1.txt,"
+                                           "cop_hat1000-1.txt,Power-Grid.txt",
+                    help="reference graph files compared with the reference's CUDA program in the default run "
+                         "('' to skip)")
     ap.add_argument("--served-seconds", type=float, default=10.0)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--stream-seconds", type=float, default=60.0)
@@ -657,6 +664,18 @@ def rank0_samples(args, recs, all_idx, local):
             "kernel_ms_sum": sum(r[3] for r in ok) if ok else None,
             "ours_plain_instances_per_s": m_ok / tm, "ours_plain_wrong": m_bad,
             "ours_plain_kernel_ms_sum": sum(s.kernel_ms for s in mine)}
+    # the same comparison on the reference's own graph files (those both sides
+    # answer within seconds; `--workload files` runs all of them)
+    if args.ref_files:
+        rows = compare_files([f for f in args.ref_files.split(",") if f], 30.0, device=local)
+        both = [r for r in rows if r.get("ours", {}).get("correct") and r.get("reference_cuda", {}).get("correct")]
+        out["reference_files"] = {
+            "files": rows,
+            "ours_correct": sum(1 for r in rows if r.get("ours", {}).get("correct")),
+            "reference_correct": sum(1 for r in rows if r.get("reference_cuda", {}).get("correct")),
+            "kernel_ms_sum_where_both_correct": {"ours": round(sum(r["ours"]["kernel_ms"] for r in both), 2),
+                                                 "reference_cuda": round(sum(r["reference_cuda"]["kernel_ms"]
+                                                                             for r in both), 2)}}
     return out
 
 
@@ -688,21 +707,18 @@ REF_CUDA_NOT_RUN = {"vc-exact_009.txt": "stack allocation of (UB+1)*n*4 bytes pe
                     "vc-exact_023.txt": "stack allocation of (UB+1)*n*4 bytes per block (~1.8 GB) fails unchecked"}
 
 
-def files_arm(args, world, rank):
+def compare_files(names, tl, device=-1):
     """The reference's graph files (test/test_graphs, known optima from
     test/runGraphs.py:8-30): this library's plain vc_solve (host buffers, no
-    upper bound given) and the reference's own CUDA program (oracle/_ref/cuda/
-    output: hybrid MVC kernel, default sizing, its CPU upper bounds first), each
-    with --file-time-limit seconds per file.  Reports per file the kernel time,
-    the call's time and whether the answer equals the known optimum."""
-    if rank != 0:
-        return
+    upper bound given; the second of two calls is reported when the first
+    solved it) and the reference's own CUDA program (oracle/_ref/cuda/output:
+    hybrid MVC kernel, default sizing, its CPU upper bounds first), each with
+    `tl` seconds per file.  Per file: kernel time, call time, and whether the
+    answer equals the known optimum."""
     import gzip
     import shutil
     import vcgpu
     known = json.load(open(os.path.join(REPO, "tests", "golden", "known_answers.json")))["mvc"]
-    names = [f for f in args.files.split(",") if f] or REF_FILES_1BASED
-    tl = args.file_time_limit
     rows = []
     for name in names:
         src = os.path.join(REPO, "oracle", "_ref", "graphs", name + ".gz")
@@ -711,15 +727,17 @@ def files_arm(args, world, rank):
             continue
         zero = name.startswith("formated_") or name.startswith("lastfm")
         g = W.read_reference_file(src, one_based=not zero)
-        r = vcgpu.solve(g, "mvc", time_limit=tl)
-        r = vcgpu.solve(g, "mvc", time_limit=tl) if r.status == vcgpu.VC_OK else r  # warm: time the second call
+        r = vcgpu.solve(g, "mvc", time_limit=tl, device=device)
+        r = vcgpu.solve(g, "mvc", time_limit=tl, device=device) if r.status == vcgpu.VC_OK else r
         ok = r.status == vcgpu.VC_OK and r.size == known[name] and W.is_cover(g, r.cover)
         ours = {"status": vcgpu.STATUS_NAMES.get(r.status, r.status), "size": r.size, "correct": bool(ok),
                 "kernel_ms": round(r.kernel_ms, 2), "call_ms": round(r.total_ms, 2), "tree_nodes": int(r.tree_nodes)}
         ref = {"unavailable": "oracle/_ref/cuda/output not built"}
         if name in REF_CUDA_NOT_RUN:
             ref = {"not_run": REF_CUDA_NOT_RUN[name]}
-        elif os.path.exists(REF_CUDA) and not zero:
+        elif zero:
+            ref = {"not_run": "0-based file (the reference's loader shifts every id down by one)"}
+        elif os.path.exists(REF_CUDA):
             with tempfile.TemporaryDirectory() as td:
                 os.makedirs(os.path.join(td, "Results"))
                 path = os.path.join(td, name)
@@ -740,9 +758,19 @@ def files_arm(args, world, rank):
                 except (OSError, IndexError, ValueError) as e:
                     ref = {"status": "error", "error": repr(e)[:120]}
         rows.append({"file": name, "n": g.n, "m": g.m, "known_opt": known[name], "ours": ours, "reference_cuda": ref})
+    return rows
+
+
+def files_arm(args, world, rank):
+    """`--workload files`: compare_files over --files (default: every 1-based
+    file), --file-time-limit seconds per file; one JSON line."""
+    if rank != 0:
+        return
+    names = [f for f in args.files.split(",") if f] or REF_FILES_1BASED
+    tl = args.file_time_limit
     line = {"metric": "reference graph files: kernel ms per file, this library vs the reference's CUDA program",
             "unit": "ms", "higher_is_better": False, "n_gpus": 1, "data": "the reference's test/test_graphs files",
-            "time_limit_s": tl, "files": rows}
+            "time_limit_s": tl, "files": compare_files(names, tl)}
     print(json.dumps(line))
 
 
