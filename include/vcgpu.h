@@ -145,6 +145,21 @@ vc_status vc_remove_max_ub(const vc_csr_arena *arena, int32_t device, uint32_t *
 vc_status vc_remove_edge_ub(const vc_csr_arena *arena, uint32_t r, int32_t device, uint32_t *ub, uint8_t *cover,
                             float *kernel_ms);
 
+/* The MCM mode: the search the reference's default build runs (`#define VC 0`,
+ * src/main.cu:9-36; GlobalWorkList_MCM.cuh:13-190 replaces the hybrid MVC
+ * kernel there).  An edge-branching search in CSR entry order: a node counts
+ * its matched and isolated vertices, takes the first entry at or after its
+ * cursor whose two vertices are unmatched and non-isolated, and branches into
+ * "match it" and "skip it"; a leaf raises the launch's maximum.  out->size
+ * receives that maximum -- 2 * (maximum matching) + (isolated vertices) once the
+ * tree is finished, the `minimum` field of the reference's Results.csv row; its
+ * CLI prints half of it as "Size of maximum matching" -- and tree_nodes /
+ * kernel_ms as vc_solve.  req->instance must be VC_MVC (the reference's MCM
+ * build refuses PVC, main.cu:155-189); graphs of up to 1024 vertices
+ * (VC_ERR_TOO_LARGE above); host input only.  VC_TIMEOUT / VC_BUDGET leave the
+ * largest count reached so far. */
+vc_status vc_mcm(const vc_csr *g, const vc_request *req, vc_result *out);
+
 /* The autotuner (replaces the reference's fixed launch-sizing rule,
  * setBlockDimAndUseGlobalMemoryAutoWorkListSize, src/auxFunctions.cpp:469-578):
  * for each size class of graphs (dense n <= 64, <= 128, <= 255; wide dense

@@ -55,6 +55,8 @@ def lib():
         L.oracle_remove_edge_ub.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _u8p]
         L.oracle_remove_edge_ub.restype = ctypes.c_uint32
         L.oracle_is_cover.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u8p]
+        L.oracle_mcm.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint64, _u32p, ctypes.POINTER(ctypes.c_uint64)]
+        L.oracle_mcm.restype = ctypes.c_int
         L.oracle_is_cover.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -111,6 +113,17 @@ def mvc(g, ub: Optional[int] = None, node_limit: int = 0):
     if not improved.value:
         cover = ub_cover
     return st, int(size.value), (cover[:g.n].astype(bool) if cover is not None else None), int(nodes.value)
+
+
+def mcm(g, node_limit: int = 0):
+    """The MCM search of the reference's default build by the restatement.
+    Returns (status, maximum, nodes); on a finished tree the maximum is
+    2 * maximum matching + isolated vertices."""
+    rp, col = _arrays(g)
+    best = ctypes.c_uint32(0)
+    nodes = ctypes.c_uint64(0)
+    st = lib().oracle_mcm(g.n, _p32(rp), _p32(col), node_limit, ctypes.byref(best), ctypes.byref(nodes))
+    return st, int(best.value), int(nodes.value)
 
 
 def pvc(g, k: int, node_limit: int = 0):

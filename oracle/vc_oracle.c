@@ -24,6 +24,8 @@
  *                  the compacted (unsorted) row, as the reference does.
  *   oracle_remove_edge_ub -> RemoveEdgeApproximateMVC exactly (auxFunctions.cpp:258-306),
  *                  with the value rand() returns after srand(time(0)) as a parameter.
+ *   oracle_mcm  -> the edge-branching search of the reference's default build
+ *                  (`#define VC 0`: GlobalWorkList_MCM.cuh:13-190), see below.
  *
  * Same rules, same order (leaf, triangle, high-degree; repeat while triangle or
  * high-degree changed), same branching (max-degree vertex, lowest index on ties;
@@ -483,4 +485,67 @@ int oracle_is_cover(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, co
         for (uint32_t e = row_ptr[v]; e < row_ptr[v + 1]; ++e)
             if (!cover[v] && !cover[col[e]]) return 0;
     return 1;
+}
+
+/* oracle_mcm -> the search of the reference's default build (`#define VC 0`,
+ * src/main.cu:9-36): GlobalWorkList_MCM.cuh:13-190 with findNextEdge
+ * (helperFunctions.cuh:86-102), skipEdge (:188-195), deleteNextEdge (:218-225)
+ * and getMatchedVertices (:532-553).  Depth first with the "match" child first
+ * and no pruning beyond the reference's own (a node whose every vertex is
+ * matched or isolated, or a maximum already equal to n, is a leaf).  A vertex
+ * is available while unmatched with degree > 0; a node counts the unavailable
+ * ones, takes the first CSR entry at or after its cursor whose row and column
+ * vertices are both available, and branches into "match both" (cursor stays at
+ * the entry, which is now ineligible) and "skip it" (cursor past the entry).
+ * Returns ORACLE_OK or ORACLE_BUDGET; *best_out = the maximum count over leaves
+ * (2 * maximum matching + isolated vertices on a finished tree). */
+int oracle_mcm(uint32_t n, const uint32_t *row_ptr, const uint32_t *col, uint64_t node_limit, uint32_t *best_out,
+               uint64_t *nodes_out)
+{
+    const uint32_t m2 = row_ptr[n];
+    uint32_t *src = (uint32_t *)malloc(sizeof(uint32_t) * (m2 ? m2 : 1));
+    uint8_t *avail = (uint8_t *)malloc(n ? n : 1);
+    uint32_t *frame = (uint32_t *)malloc(sizeof(uint32_t) * (n / 2 + 1));
+    uint32_t avc = 0, best = 0, level = 0, cursor = 0;
+    uint64_t nodes = 0;
+    int status = ORACLE_OK;
+    for (uint32_t v = 0; v < n; ++v) {
+        for (uint32_t e = row_ptr[v]; e < row_ptr[v + 1]; ++e) src[e] = v;
+        avail[v] = row_ptr[v + 1] > row_ptr[v];
+        avc += avail[v];
+    }
+    for (;;) {
+        ++nodes;
+        if (node_limit && nodes > node_limit) {
+            status = ORACLE_BUDGET;
+            break;
+        }
+        const uint32_t cnt = n - avc;
+        uint32_t next = m2;
+        if (cnt < n && best < n)
+            for (uint32_t e = cursor; e < m2; ++e)
+                if (avail[src[e]] && avail[col[e]]) {
+                    next = e;
+                    break;
+                }
+        if (next < m2) {  /* match the entry's two vertices; the skip child waits on the frame */
+            frame[level++] = next;
+            avail[src[next]] = avail[col[next]] = 0;
+            avc -= 2;
+            cursor = next;
+            continue;
+        }
+        if (cnt > best) best = cnt;  /* a leaf */
+        if (level == 0) break;
+        const uint32_t e = frame[--level];  /* the skip child of the deepest matched entry */
+        avail[src[e]] = avail[col[e]] = 1;
+        avc += 2;
+        cursor = e + 1;
+    }
+    free(src);
+    free(avail);
+    free(frame);
+    *best_out = best;
+    if (nodes_out) *nodes_out = nodes;
+    return status;
 }

@@ -59,6 +59,7 @@ struct Config {
     const char *graphFileName = "GraphInput.txt";
     bool zeroBased = false;  // -z: vertex ids in the file start at 0
     bool upperBounds = false;  // -u: the reference's two upper-bound heuristics, on the GPU
+    bool mcm = false;          // -M: the MCM search of the reference's default (`VC 0`) build
 };
 
 void usage()
@@ -79,7 +80,9 @@ void usage()
             "   -g <Use Global Mem>   recorded; the library picks shared or global workspaces\n"
             "   -n <Number of Blocks> recorded; the library sizes the persistent grid\n"
             "   -z                    vertex ids in the graph file start at 0 (the formated_* inputs)\n"
-            "   -u                    also run the RemoveMax / RemoveEdge upper-bound heuristics (on the GPU)\n\n");
+            "   -u                    also run the RemoveMax / RemoveEdge upper-bound heuristics (on the GPU)\n"
+            "   -M                    run the MCM search of the reference's default build (VC 0): prints the\n"
+            "                         size of maximum matching (mvc, hybrid only; graphs of up to 1024 vertices)\n\n");
 }
 
 const char *asString(Version v) { return v == STACK_ONLY ? "stackonly" : (v == HYBRID ? "hybrid" : "sequential"); }
@@ -89,7 +92,7 @@ Config parseArgs(int argc, char **argv)
 {
     Config c;
     int opt;
-    while ((opt = getopt(argc, argv, "v:f:o:i:k:q:t:d:b:g:n:hzu")) >= 0) {
+    while ((opt = getopt(argc, argv, "v:f:o:i:k:q:t:d:b:g:n:hzuM")) >= 0) {
         switch (opt) {
         case 'v':
             if (!strcmp(optarg, "stackonly")) c.version = STACK_ONLY;
@@ -113,6 +116,7 @@ Config parseArgs(int argc, char **argv)
         case 'n': c.numBlocks = (unsigned)atoi(optarg); break;
         case 'z': c.zeroBased = true; break;
         case 'u': c.upperBounds = true; break;
+        case 'M': c.mcm = true; break;
         case 'h': usage(); exit(0);
         default: fprintf(stderr, "\nUnrecognized option!\n"); exit(0);
         }
@@ -259,6 +263,10 @@ int main(int argc, char **argv)
         fprintf(stderr, "-v sequential: the CPU solver is not part of this build; use -v hybrid\n");
         return 1;
     }
+    if (config.mcm && (config.version != HYBRID || config.instance != MVC)) {  // main.cu:155-189
+        printf("unsupported version %d instance %d\n", (int)config.version, (int)config.instance);
+        return 1;
+    }
     uint32_t n = 0, m = 0;
     std::vector<uint32_t> rp, col;
     std::string err;
@@ -312,6 +320,22 @@ int main(int argc, char **argv)
     vc_result res;
     memset(&res, 0, sizeof(res));
     res.cover_mask = cover.data();
+    if (config.mcm) {  // main.cu:9-36 (`VC 0`): the maximum starts at 0 (main.cu:240)
+        res.cover_mask = nullptr;
+        vc_status st = vc_mcm(&g, &req, &res);
+        if (st != VC_OK) {
+            fprintf(stderr, "GPU Error: %s\n", vc_status_string(st));
+            return 1;
+        }
+        uint32_t shape[5] = {0, 0, 0, 0, 0};
+        vc_debug_stats(0, -1, nullptr, 0, shape);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+        printf("\nElapsed time: %fms \n", res.kernel_ms);
+        printResults(config, n, m, res.size, 0, res.kernel_ms, shape, sms, bounds);
+        printf("\nSize of maximum matching: %u\n\n", res.size / 2);
+        return 0;
+    }
     const char *counters_env = getenv("VC_COUNTERS");
     const bool counters = counters_env && counters_env[0] == '1';
     if (counters) vc_debug_stats(0, 1, nullptr, 0, nullptr);
@@ -329,7 +353,8 @@ int main(int argc, char **argv)
     printf("NumOfBlocks : %u\n", shape[0]);
     printf("NumOfSearchUnits : %u\n\n", shape[3]);
     printf("Elapsed time: %fms \n", res.kernel_ms);
-    printResults(config, n, m, res.size, res.decision, res.kernel_ms, shape, sms, bounds);
+    // kFound is the PVC answer; an MVC row keeps it at 0 (main.cu:80, 355-359)
+    printResults(config, n, m, res.size, config.instance == PVC ? res.decision : 0, res.kernel_ms, shape, sms, bounds);
     if (counters) printCounters(config, sms);
     if (config.instance == PVC) {
         if (res.decision) printf("\nMinimum is less than or equal to K: %u\n\n", config.k);

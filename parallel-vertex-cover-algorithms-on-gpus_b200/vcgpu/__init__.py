@@ -93,6 +93,9 @@ def lib():
         L.vc_debug_stats.restype = ctypes.c_uint32
         L.vc_status_string.argtypes = [ctypes.c_int]
         L.vc_status_string.restype = ctypes.c_char_p
+        if hasattr(L, "vc_mcm"):
+            L.vc_mcm.argtypes = [ctypes.POINTER(Csr), ctypes.POINTER(Request), ctypes.POINTER(Result)]
+            L.vc_mcm.restype = ctypes.c_int
         if hasattr(L, "vc_solve_noalloc"):
             L.vc_solve_noalloc.argtypes = [ctypes.POINTER(Csr), ctypes.POINTER(Request), ctypes.c_void_p,
                                            ctypes.c_void_p]
@@ -164,6 +167,21 @@ def solve(g, instance: str = "mvc", k: int = 0, ub: int = 0, node_limit: int = 0
     if st in (VC_ERR_INVALID, VC_ERR_CUDA, VC_ERR_NOMEM, VC_ERR_TOO_LARGE, VC_ERR_NO_DEVICE):
         return Solution(st, 0, 0, None, 0, 0.0, 0.0)
     return _solution(res, cover[:g.n] if cover is not None else None, g.n)
+
+
+def mcm(g, node_limit: int = 0, time_limit: float = 0.0, device: int = -1) -> Solution:
+    """The MCM mode (vc_mcm): size = 2 * maximum matching + isolated vertices,
+    the reference's default build's `maximum`."""
+    rp = np.ascontiguousarray(g.row_ptr, dtype=np.uint32)
+    col = np.ascontiguousarray(g.col, dtype=np.uint32)
+    c = Csr(g.n, col.shape[0] // 2, rp.ctypes.data, col.ctypes.data if col.size else None, None)
+    req = _request("mvc", 0, 0, node_limit, time_limit, 0, device)
+    res = Result()
+    st = lib().vc_mcm(ctypes.byref(c), ctypes.byref(req), ctypes.byref(res))
+    if st in (VC_ERR_INVALID, VC_ERR_CUDA, VC_ERR_NOMEM, VC_ERR_TOO_LARGE, VC_ERR_NO_DEVICE):
+        return Solution(st, 0, 0, None, 0, 0.0, 0.0)
+    return Solution(int(res.status), int(res.size), int(res.decision), None, int(res.tree_nodes),
+                    float(res.kernel_ms), float(res.total_ms), 0.0)
 
 
 def solve_device(n: int, m: int, d_row_ptr: int, d_col: int, instance: str = "mvc", k: int = 0, ub: int = 0,

@@ -101,6 +101,17 @@ def gnp(n: int, p: float, seed: int, name: str = "") -> Graph:
     return from_edges(n, _distinct_pairs(rng, n, m), name or f"gnp_n{n}_p{p:.4f}_s{seed}")
 
 
+def planted_matching(n: int, d: float, seed: int, name: str = "") -> Graph:
+    """The pairs (2i, 2i+1) plus uniform random edges up to average degree d:
+    a graph whose maximum matching is known (n // 2 pairs) and is the first one
+    an in-order greedy matching finds (the MCM mode's large test graphs)."""
+    rng = np.random.default_rng(seed)
+    pairs = np.stack([np.arange(0, n - 1, 2), np.arange(1, n, 2)], axis=1)
+    extra = _distinct_pairs(rng, n, max(0, int(n * d / 2) - len(pairs)))
+    return from_edges(n, np.concatenate([pairs, extra]) if len(extra) else pairs,
+                      name or f"planted_matching_n{n}_d{d}_s{seed}")
+
+
 def random_regular(n: int, d: int, seed: int, name: str = "") -> Graph:
     """Uniform random d-regular simple graph by the pairing model with rejection."""
     if (n * d) % 2 or d >= n:

@@ -11,6 +11,7 @@ carry no answer and are left out of parity claims).
     python tests/golden/make_golden.py batch-hard [--workers 6]   # the "budget" ones, no limit
     python tests/golden/make_golden.py stream [--count 2000] [--limit 20000000]
     python tests/golden/make_golden.py files      # reference known-answer graph files
+    python tests/golden/make_golden.py mcm        # the MCM mode's answers (needs networkx)
 
 Output files are JSON (lines for the long runs, so partial runs are usable).
 Workers are started with the `spawn` method.
@@ -138,9 +139,57 @@ def files():
     print(golden)
 
 
+def _mcm_graph(spec):
+    from vcgpu import workloads as W
+    if spec["family"] == "gnp":
+        return W.gnp(spec["n"], spec["d"] / (spec["n"] - 1), spec["seed"])
+    return W.planted_matching(spec["n"], spec["d"], spec["seed"])
+
+
+def mcm():
+    """Answers of the MCM mode (the search of the reference's default build):
+    2 * maximum matching + isolated vertices, from networkx's maximum-cardinality
+    matching.  The search is exhaustive (exponential in the edges), so the
+    graphs are the ones it can finish: G(n, p) graphs on which the oracle's
+    restatement (no cut at all) finishes within 3e7 tree nodes and agrees, and
+    planted-matching graphs of up to 1024 vertices whose maximum matching is the
+    first one the in-order search meets (odd n: one vertex unmatched, which the
+    search's bound then proves at once)."""
+    import networkx as nx
+    import oracle as O
+    specs = [{"family": "gnp", "n": n, "d": d, "seed": 700 + i}
+             for i, (n, d) in enumerate([(6, 2.0), (8, 1.5), (9, 3.0), (10, 2.5), (11, 4.0), (12, 1.2), (13, 3.0),
+                                          (14, 2.0), (15, 5.0), (16, 2.5), (17, 3.5), (18, 1.8), (18, 4.0),
+                                          (22, 2.5), (26, 3.0), (30, 2.0), (34, 3.5), (40, 2.5), (48, 3.0)])]
+    specs += [{"family": "planted", "n": n, "d": 6.0, "seed": 800 + i}
+              for i, n in enumerate([64, 101, 256, 511, 640, 1023, 1024])]
+    out = []
+    for sp in specs:
+        g = _mcm_graph(sp)
+        G = nx.Graph()
+        G.add_nodes_from(range(g.n))
+        for u in range(g.n):
+            for v in g.col[g.row_ptr[u]:g.row_ptr[u + 1]]:
+                if u < v:
+                    G.add_edge(u, int(v))
+        nu = len(nx.max_weight_matching(G, maxcardinality=True))
+        iso = sum(1 for v in range(g.n) if G.degree(v) == 0)
+        rec = dict(sp, m=g.m, matching=nu, isolated=iso, expect=2 * nu + iso)
+        if sp["family"] == "gnp":
+            st, best, nodes = O.mcm(g, node_limit=30_000_000)
+            if st != O.OK:
+                continue
+            assert best == rec["expect"], (sp, best, rec["expect"])
+            rec["oracle_nodes"] = nodes
+        out.append(rec)
+    with open(os.path.join(HERE, "mcm.json"), "w") as f:
+        json.dump(out, f, indent=0)
+    print(len(out), [(r["family"], r["n"], r["expect"], r.get("oracle_nodes")) for r in out])
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["small", "batch", "batch-hard", "stream", "files"])
+    ap.add_argument("what", choices=["small", "batch", "batch-hard", "stream", "files", "mcm"])
     ap.add_argument("--count", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--limit", type=int, default=100_000_000)
@@ -150,6 +199,8 @@ def main():
         small()
     elif a.what == "files":
         files()
+    elif a.what == "mcm":
+        mcm()
     elif a.what == "batch":
         _run_pool(_batch_job, [(i, a.seed, a.limit) for i in range(a.count)],
                   os.path.join(HERE, f"batch_seed{a.seed}.jsonl"), a.workers)

@@ -149,3 +149,50 @@ def test_upper_bound_restatements_match_reference():
             assert W.is_cover(g, cover_e) and int(cover_e.sum()) == ub_e
             compared += 1
     assert compared >= 100
+
+
+def _max_matching_brute(g):
+    """Largest matching by trying edge subsets in order (tiny graphs only)."""
+    edges = [(u, int(v)) for u in range(g.n) for v in g.col[g.row_ptr[u]:g.row_ptr[u + 1]] if u < v]
+    best = 0
+
+    def rec(i, used, size):
+        nonlocal best
+        best = max(best, size)
+        if i == len(edges) or size + (g.n - len(used)) // 2 <= best:
+            return
+        u, v = edges[i]
+        if u not in used and v not in used:
+            rec(i + 1, used | {u, v}, size + 1)
+        rec(i + 1, used, size)
+
+    rec(0, frozenset(), 0)
+    return best
+
+
+def test_mcm_restatement_equals_twice_the_maximum_matching_plus_isolated():
+    """The MCM search of the reference's default build (oracle_mcm) finishes at
+    2 * maximum matching + isolated vertices: checked against a maximum
+    matching found by brute force (and by networkx where it is installed)."""
+    nx = None
+    try:
+        import networkx as nx  # noqa: F811
+    except ImportError:
+        pass
+    rng = np.random.default_rng(17)
+    for _ in range(120):
+        n = int(rng.integers(1, 14))
+        g = W.gnp(n, float(rng.uniform(0.05, 0.6)), int(rng.integers(1 << 30)))
+        st, best, nodes = O.mcm(g)
+        assert st == O.OK and nodes >= 1
+        iso = int(np.sum(np.diff(g.row_ptr) == 0))
+        assert best == 2 * _max_matching_brute(g) + iso
+        if nx is not None:
+            G = nx.Graph()
+            G.add_nodes_from(range(n))
+            G.add_edges_from((u, int(v)) for u in range(n) for v in g.col[g.row_ptr[u]:g.row_ptr[u + 1]] if u < v)
+            assert best == 2 * len(nx.max_weight_matching(G, maxcardinality=True)) + iso
+    # the node budget stops the search
+    g = W.gnp(40, 3.0 / 39, 5)
+    st, _, nodes = O.mcm(g, node_limit=1000)
+    assert st == O.BUDGET and nodes == 1001
