@@ -36,6 +36,8 @@ set); `--set full` runs all 4096.
 alone for longer; `--workload ub` the upper-bound heuristics; `--workload files`
 the reference's own graph files (staged by `make -C oracle graphs`) through
 vc_solve beside the reference's own CUDA program on the same files; `--workload
+mcm` the MCM mode (vc_mcm) beside the reference's default `VC 0` build on the
+graphs of tests/golden/mcm.json; `--workload
 profile` is the torch-free case for profiler captures: the first --count graphs
 of the step's set in one vc_solve_batch call, --reps times.
 
@@ -79,7 +81,7 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub", "profile", "files"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "stream", "ub", "profile", "files", "mcm"])
     ap.add_argument("--files", default="",
                     help="--workload files: comma-separated reference graph files (default: the 1-based ones)")
     ap.add_argument("--file-time-limit", type=float, default=30.0,
@@ -774,6 +776,53 @@ def files_arm(args, world, rank):
     print(json.dumps(line))
 
 
+REF_CUDA_MCM = os.path.join(REPO, "oracle", "_ref", "cuda_mcm", "output")
+
+
+def mcm_arm(args, world, rank):
+    """The MCM mode: vc_mcm against the reference's own default build
+    (oracle/_ref/cuda_mcm/output, `#define VC 0`, one process per graph) on the
+    graphs of tests/golden/mcm.json, whose answers (2 * maximum matching +
+    isolated vertices) come from maximum-cardinality matchings.  The reference
+    runs --file-time-limit seconds per graph."""
+    if rank != 0:
+        return
+    import vcgpu
+    recs = json.load(open(os.path.join(REPO, "tests", "golden", "mcm.json")))
+    rows = []
+    for r in recs:
+        g = (W.gnp(r["n"], r["d"] / (r["n"] - 1), r["seed"]) if r["family"] == "gnp"
+             else W.planted_matching(r["n"], r["d"], r["seed"]))
+        s = vcgpu.mcm(g, time_limit=60.0)
+        s = vcgpu.mcm(g, time_limit=60.0) if s.status == vcgpu.VC_OK else s
+        row = {"graph": f"{r['family']} n={r['n']} d={r['d']} seed={r['seed']}", "expect": r["expect"],
+               "ours": {"status": vcgpu.STATUS_NAMES.get(s.status, s.status), "maximum": s.size,
+                        "correct": s.status == vcgpu.VC_OK and s.size == r["expect"],
+                        "kernel_ms": round(s.kernel_ms, 3), "tree_nodes": s.tree_nodes}}
+        if os.path.exists(REF_CUDA_MCM):
+            with tempfile.TemporaryDirectory() as td:
+                os.makedirs(os.path.join(td, "Results"))
+                path = os.path.join(td, "g.txt")
+                W.write_reference_file(g, path)
+                t0 = time.perf_counter()
+                try:
+                    p = subprocess.run([REF_CUDA_MCM, "-f", path, "-o", "mcm"], cwd=td, capture_output=True,
+                                       text=True, timeout=args.file_time_limit)
+                    f = open(os.path.join(td, "Results", "Results.csv")).read().strip().splitlines()[-1].split(",")
+                    row["reference_cuda"] = {"status": "ok" if p.returncode == 0 else f"exit {p.returncode}",
+                                             "maximum": int(f[18]), "correct": int(f[18]) == r["expect"],
+                                             "kernel_ms": float(f[21]),
+                                             "process_s": round(time.perf_counter() - t0, 2)}
+                except subprocess.TimeoutExpired:
+                    row["reference_cuda"] = {"status": "timeout", "process_s": args.file_time_limit}
+                except (OSError, IndexError, ValueError) as e:
+                    row["reference_cuda"] = {"status": "error", "error": repr(e)[:120]}
+        rows.append(row)
+    print(json.dumps({"metric": "MCM mode: kernel ms per graph, this library vs the reference's default build",
+                      "unit": "ms", "higher_is_better": False, "n_gpus": 1, "data": "synthetic (tests/golden/mcm.json)",
+                      "graphs": rows}))
+
+
 def ub_arm(args, world, rank):
     """The reference's upper-bound heuristics on the GPU (vc_remove_max_ub /
     vc_remove_edge_ub): Chung-Lu n=100000 (one graph) and the 4096 batched
@@ -859,6 +908,8 @@ def main():
             ub_arm(args, world, rank)
         elif args.workload == "files":
             files_arm(args, world, rank)
+        elif args.workload == "mcm":
+            mcm_arm(args, world, rank)
         else:
             our_arm(args, world, rank, local, pg)
     finally:
