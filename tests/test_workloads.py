@@ -63,3 +63,17 @@ def test_chung_lu_small():
     g = W.chung_lu(n=3000, gamma=2.1, avg_deg=8, max_deg=200, seed=7)
     _simple(g)
     assert g.degrees().max() <= 400
+
+
+def test_planted_matching_holds_its_pairs():
+    """The MCM mode's large test graphs: every pair (2i, 2i+1) is an edge, so the
+    maximum matching has n // 2 pairs, and the extra edges bring the average
+    degree near d."""
+    for n, d, seed in ((64, 6.0, 1), (101, 4.0, 2), (1024, 6.0, 3)):
+        g = W.planted_matching(n, d, seed)
+        assert g.n == n
+        for i in range(0, n - 1, 2):
+            row = g.col[g.row_ptr[i]:g.row_ptr[i + 1]]
+            assert i + 1 in row
+        assert abs(2 * g.m / n - d) < 1.0
+        assert W.planted_matching(n, d, seed).m == g.m  # seeded
