@@ -264,8 +264,10 @@ __global__ void __launch_bounds__(NT) k_mcm(Params P, McmArgs A)
             c_best = __shfl_sync(0xffffffffu, nb, 0);
         }
         if (descend) {
-            // share the shallowest untried skip child while more units wait than records are queued
-            if (bot < level && (long long)(uint32_t)c_state - (long long)(c_state >> 32) > 0 &&
+            // share the shallowest untried skip child while more units wait than records are
+            // queued, once a first leaf has set a maximum: the first descent is a greedy
+            // matching, often already maximum, and runs fastest with the SMs to itself
+            if (c_best > 0 && bot < level && (long long)(uint32_t)c_state - (long long)(c_state >> 32) > 0 &&
                 mcm_donate(P, A, st, fe, fp, bot, level, av, lane)) {
                 bot += 1;
                 c_state += 1ull << 32;
