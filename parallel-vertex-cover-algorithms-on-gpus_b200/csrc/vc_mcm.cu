@@ -369,7 +369,15 @@ extern "C" vc_status vc_mcm(const vc_csr *g, const vc_request *req, vc_result *o
         cudaStreamSynchronize(stream);
         return VC_ERR_CUDA;
     }
-    k_mcm_init_ring<<<(q + 255) / 256, 256, 0, stream>>>((unsigned long long *)c->seq.p, q);
+    // launches are checked by their own return codes: an error the caller left
+    // pending is neither reported here nor cleared
+    unsigned long long *seq = (unsigned long long *)c->seq.p;
+    void *init_args[] = {&seq, &q};
+    if (cudaLaunchKernel((const void *)k_mcm_init_ring, dim3((q + 255) / 256), dim3(256), init_args, 0, stream) !=
+        cudaSuccess) {
+        cudaStreamSynchronize(stream);
+        return VC_ERR_CUDA;
+    }
     Params P;
     memset(&P, 0, sizeof(P));
     P.row_ptr = (const uint32_t *)c->rp.p;
@@ -398,13 +406,14 @@ extern "C" vc_status vc_mcm(const vc_csr *g, const vc_request *req, vc_result *o
     c->last_plan = pl;  // reported by vc_debug_stats
     c->last_num_su = 0;
     cudaEventRecord(c->ev0, stream);
-    fn<<<grid, kMcmThreads, smem, stream>>>(P, A);
+    void *args[] = {&P, &A};
+    const bool launched =
+        cudaLaunchKernel((const void *)fn, dim3(grid), dim3(kMcmThreads), args, smem, stream) == cudaSuccess;
     cudaEventRecord(c->ev1, stream);
     g_launches += 2;
     InstState s1;
     unsigned long long abort_word = 0;
-    ok = cudaGetLastError() == cudaSuccess &&
-         cudaMemcpyAsync(&s1, c->st.p, sizeof(s1), cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
+    ok = launched && cudaMemcpyAsync(&s1, c->st.p, sizeof(s1), cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
          cudaMemcpyAsync(&abort_word, (unsigned long long *)c->ctl.p + kAbort, sizeof(abort_word),
                          cudaMemcpyDeviceToHost, stream) == cudaSuccess;
     if (cudaStreamSynchronize(stream) != cudaSuccess || !ok) return VC_ERR_CUDA;

@@ -413,10 +413,11 @@ vc_status ub_run(const vc_csr_arena *a, uint32_t mode, uint32_t r, int32_t devic
     P.mode = mode;
     P.r = r;
     cudaEventRecord(c->ev0, st);
-    k_ub<<<count, kUbThreads, 0, st>>>(P);
+    void *args[] = {&P};
+    // checked by its own return code: an error the caller left pending is neither reported nor cleared
+    bool good = cudaLaunchKernel((const void *)k_ub, dim3(count), dim3(kUbThreads), args, 0, st) == cudaSuccess;
     cudaEventRecord(c->ev1, st);
     g_launches += 1;
-    bool good = cudaGetLastError() == cudaSuccess;
     good = good && cudaMemcpyAsync(ub, d_ub.p, 4ull * count, cudaMemcpyDeviceToHost, st) == cudaSuccess;
     std::vector<int32_t> deg;
     if (cover && good) {
