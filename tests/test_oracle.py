@@ -196,3 +196,26 @@ def test_mcm_restatement_equals_twice_the_maximum_matching_plus_isolated():
     g = W.gnp(40, 3.0 / 39, 5)
     st, _, nodes = O.mcm(g, node_limit=1000)
     assert st == O.BUDGET and nodes == 1001
+
+
+def test_hard_batch_fixture_is_consistent():
+    """tests/golden/batch_seed0_hard.jsonl (the batched graphs the budgeted
+    oracle run left open, solved without a limit) describes the same graphs as
+    the main fixture, never exceeds the cover it started from, and pins each
+    graph (a graph solved twice has one answer)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "batch_seed0_hard.jsonl")
+    if not os.path.exists(path):
+        pytest.skip("no hard fixture yet")
+    main = {r["i"]: r for r in (json.loads(l) for l in open(os.path.join(os.path.dirname(path), "batch_seed0.jsonl"))
+                                if l.strip())}
+    seen = {}
+    for line in open(path):
+        if not line.strip():
+            continue
+        r = json.loads(line)
+        assert seen.setdefault(r["i"], r["opt"]) == r["opt"]
+        m = main[r["i"]]
+        assert m["status"] != "ok" and (r["n"], r["m"]) == (m["n"], m["m"])
+        assert r["status"] == "ok" and r["opt"] <= r["ub_start"] == m["ub"]
+        g = W.batch_instance(r["i"])
+        assert (g.n, g.m) == (r["n"], r["m"])
